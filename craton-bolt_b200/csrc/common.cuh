@@ -1,0 +1,140 @@
+// common.cuh — shared device/host helpers of the bolt-b200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bolt_b200.h"
+
+typedef unsigned long long ull;
+typedef long long ll;
+
+namespace bolt {
+
+// ---- device status word bits (read back by the host after a call) --------
+enum : uint32_t {
+    ST_FLAG_SPILL = 1u << 0,     // global hash table probe limit reached
+    ST_FLAG_OVERFLOW = 1u << 1,  // integer / decimal SUM out of range
+    ST_FLAG_RANGE = 1u << 2,     // f64 SUM value outside the fixed-point window
+    ST_FLAG_TIMEOUT = 1u << 3,   // bounded spin gave up
+    ST_FLAG_DUPKEY = 1u << 4,    // duplicate join build key
+    ST_FLAG_GROW = 1u << 5,      // table occupancy over the load limit
+    ST_FLAG_DECRANGE = 1u << 6,  // decimal value does not fit the 64-bit fast path
+    ST_FLAG_CAPACITY = 1u << 7,  // output capacity exceeded
+    ST_FLAG_DECOVERFLOW = 1u << 8,  // SUM(Decimal128) outside the i128 range
+};
+
+// ---- bit-level helpers ----------------------------------------------------
+__host__ __device__ __forceinline__ int ceil_log2_u64(uint64_t x) {
+    int r = 0;
+    while ((1ull << r) < x && r < 63) ++r;
+    return r;
+}
+
+__device__ __forceinline__ bool bit_valid(const uint8_t* v, uint64_t i) {
+    return v == nullptr || ((__ldg(v + (i >> 3)) >> (i & 7)) & 1);
+}
+
+__device__ __forceinline__ void set_bit_atomic(uint8_t* bm, uint64_t i, bool on) {
+    // Byte-granular bitmap writes from different threads need atomics on the
+    // containing 32-bit word.
+    uint32_t* w = reinterpret_cast<uint32_t*>(reinterpret_cast<uintptr_t>(bm + (i >> 3)) & ~uintptr_t(3));
+    uint32_t shift = ((reinterpret_cast<uintptr_t>(bm + (i >> 3)) & 3) * 8) + (i & 7);
+    if (on) atomicOr(w, 1u << shift);
+    else atomicAnd(w, ~(1u << shift));
+}
+
+// Canonicalised float bit patterns (-0.0 -> +0.0, any NaN -> one quiet NaN),
+// the GROUP BY / JOIN / ORDER BY float key equivalence of the reference.
+__device__ __forceinline__ uint64_t canon_f64_bits(double x) {
+    if (x != x) return 0x7FF8000000000000ull;
+    if (x == 0.0) return 0ull;
+    return (uint64_t)__double_as_longlong(x);
+}
+__device__ __forceinline__ uint32_t canon_f32_bits(float x) {
+    if (x != x) return 0x7FC00000u;
+    if (x == 0.0f) return 0u;
+    return (uint32_t)__float_as_uint(x);
+}
+
+// Order-preserving u64 image of a float64 (NaN largest, -0 == +0).
+__device__ __forceinline__ uint64_t f64_order_key(double x) {
+    uint64_t b = canon_f64_bits(x);
+    uint64_t mask = (uint64_t)(((int64_t)b) >> 63) | 0x8000000000000000ull;
+    return b ^ mask;
+}
+__device__ __forceinline__ double f64_from_order_key(uint64_t k) {
+    uint64_t b = (k & 0x8000000000000000ull) ? (k ^ 0x8000000000000000ull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+// Streaming loads: evict-first so the hash tables keep L2.
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+
+// Volatile (L2-coherent) 64-bit read of a word other threads update atomically.
+__device__ __forceinline__ ull ld_volatile(const ull* p) {
+    return *reinterpret_cast<const volatile ull*>(p);
+}
+
+// Lane helpers.
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Signed 128-bit fixed-point -> correctly rounded double, times 2^-e.
+// Round-to-nearest-even on the 128-bit magnitude, then an exact power-of-two
+// scale. (Values here stay in the normal range of double.)
+__device__ __forceinline__ double i128_to_double_scaled(ull lo, ll hi, int e) {
+    bool neg = hi < 0;
+    unsigned __int128 mag = ((unsigned __int128)(ull)hi << 64) | lo;
+    if (neg) mag = (unsigned __int128)0 - mag;
+    if (mag == 0) return 0.0;
+    ull mhi = (ull)(mag >> 64), mlo = (ull)mag;
+    int top = mhi ? 127 - __clzll((ll)mhi) : 63 - __clzll((ll)mlo);
+    double d;
+    int shift = 0;
+    if (top <= 52) {
+        d = (double)mlo;  // exact
+    } else {
+        shift = top - 52;
+        unsigned __int128 mant = mag >> shift;
+        unsigned __int128 rem = mag - (mant << shift);
+        unsigned __int128 half = (unsigned __int128)1 << (shift - 1);
+        if (rem > half || (rem == half && ((ull)mant & 1ull))) mant += 1;
+        d = (double)(ull)mant;  // <= 2^53, exact
+    }
+    d = scalbn(d, shift - e);
+    return neg ? -d : d;
+}
+
+// float64 -> round-half-away 128-bit fixed point with e fractional bits.
+// Returns false for non-finite values or |v| >= 2^32 (the window the scale
+// was chosen for).
+__device__ __forceinline__ bool f64_to_fixed(double v, int e, ull& lo, ll& hi) {
+    ull b = (ull)__double_as_longlong(v);
+    int E = (int)((b >> 52) & 0x7FF);
+    ull m = b & ((1ull << 52) - 1);
+    if (E == 0x7FF) return false;
+    if (E == 0) {
+        if (m == 0) { lo = 0; hi = 0; return true; }
+        E = 1;
+    } else {
+        m |= 1ull << 52;
+    }
+    if (E - 1023 >= 32) return false;
+    int s = E - 1075 + e;
+    unsigned __int128 mag;
+    if (s >= 0) mag = (unsigned __int128)m << s;
+    else if (s > -63) mag = (unsigned __int128)((m + (1ull << (-s - 1))) >> (-s));
+    else mag = 0;
+    if (b >> 63) mag = (unsigned __int128)0 - mag;
+    lo = (ull)mag;
+    hi = (ll)(ull)(mag >> 64);
+    return true;
+}
+
+}  // namespace bolt

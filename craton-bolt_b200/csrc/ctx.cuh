@@ -1,0 +1,85 @@
+// ctx.cuh — bolt_ctx: device, scratch arena, status word, timing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "common.cuh"
+
+struct bolt_ctx {
+    int device = 0;
+    int num_sms = 148;
+    int max_smem_optin = 0;
+    // Scratch arena: a bump allocator reset at the start of every call. All
+    // kernels of one call are ordered on one stream, so reuse across calls is
+    // safe without frees.
+    char* arena = nullptr;
+    uint64_t arena_bytes = 0;
+    uint64_t arena_used = 0;
+    uint64_t arena_pinned = 0;   // bytes at the arena's start kept across calls (join tables)
+    // Device status block: [0] status flags (u32), [2..] per-call counters.
+    uint32_t* d_status = nullptr;
+    ull* d_words = nullptr;      // 64 general device words (counts, reductions)
+    ull* h_words = nullptr;      // pinned host mirror
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Ring of event pairs around the dominant kernel of profiled calls.
+    static constexpr uint32_t KRING = 256;
+    cudaEvent_t kev[2 * KRING] = {};
+    uint32_t kcount = 0;
+    double last_ms = 0.0;
+    uint32_t last_launches = 0;
+    uint32_t async_pending = 0;
+    std::string last_error;
+};
+
+namespace bolt {
+
+// Records a failure message and returns the status.
+bolt_status fail(bolt_ctx* ctx, bolt_status s, const char* fmt, ...);
+
+// Maps a CUDA error to BOLT_ERR_CUDA with its message.
+bolt_status cuda_fail(bolt_ctx* ctx, cudaError_t e, const char* where);
+
+#define BOLT_CUDA(ctx, call)                                   \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return bolt::cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+// Arena allocation (256-byte aligned); returns nullptr when exhausted.
+void* arena_alloc(bolt_ctx* ctx, uint64_t bytes);
+inline void arena_reset(bolt_ctx* ctx) { ctx->arena_used = ctx->arena_pinned; }
+
+// Begins / ends a call: resets the arena, clears the status word, records the
+// profiling event.
+bolt_status call_begin(bolt_ctx* ctx, uint32_t flags, cudaStream_t s);
+bolt_status call_end(bolt_ctx* ctx, uint32_t flags, cudaStream_t s);
+
+// Event pair around the dominant kernel of a profiled call.
+inline void kernel_mark_begin(bolt_ctx* ctx, uint32_t flags, cudaStream_t s) {
+    if ((flags & BOLT_FLAG_PROFILE) && ctx->kcount < bolt_ctx::KRING) cudaEventRecord(ctx->kev[2 * ctx->kcount], s);
+}
+inline void kernel_mark_end(bolt_ctx* ctx, uint32_t flags, cudaStream_t s) {
+    if ((flags & BOLT_FLAG_PROFILE) && ctx->kcount < bolt_ctx::KRING) {
+        cudaEventRecord(ctx->kev[2 * ctx->kcount + 1], s);
+        ctx->kcount++;
+    }
+}
+
+// Reads the status word + n device words into ctx->h_words (synchronises s).
+bolt_status read_status(bolt_ctx* ctx, cudaStream_t s, int n_words, uint32_t* flags);
+
+// Translates device status flags into a bolt_status + message.
+bolt_status flags_to_status(bolt_ctx* ctx, uint32_t flags, const char* op);
+
+inline unsigned grid_for(uint64_t n, unsigned block, unsigned max_blocks) {
+    uint64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > max_blocks) g = max_blocks;
+    return (unsigned)g;
+}
+
+}  // namespace bolt

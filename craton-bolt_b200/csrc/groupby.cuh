@@ -1,0 +1,134 @@
+// groupby.cuh — hash GROUP BY plan, kernels and host entry shared with the
+// batched / served forms.
+#pragma once
+
+#include "ctx.cuh"
+
+namespace bolt {
+
+// Per-group state kinds (8-byte words inside a hash slot). Every state's
+// identity is all-zero words, so a table is initialised with one memset.
+enum StKind : int32_t {
+    K_COUNT = 0,      // 1 word: count of valid inputs (or rows)
+    K_SUM_I32 = 1,    // 1 word: i64 sum of i32 inputs
+    K_SUM_I64 = 2,    // 2 words: sum of low 32 bits (u64), sum of high 32 bits (i64)
+    K_SUM_FX = 3,     // 2 words: i128 fixed-point sum (lo with carry, hi)
+    K_SUM_FATOM = 4,  // 1 word: f64 atomicAdd (fallback for non-finite / huge values)
+    K_MAX_ORD = 5,    // 1 word: max of an order-preserving u64 image
+    K_MIN_ORD = 6,    // 1 word: max of the bitwise NOT of that image
+    K_SUM_D64 = 7,    // 2 words: like K_SUM_I64 over Decimal128 values that fit in i64
+    K_SUM_D128 = 8,   // 3 words: low word with carry, low half of the high words + carries,
+                      // signed high half of the high words (exact 192-bit sum)
+};
+
+constexpr int GB_MAX_STATES = 8;
+constexpr int GB_MAX_PREDS = 4;
+constexpr int GB_MAX_AGGS = 16;
+
+struct StateDesc {
+    const void* col;
+    const uint8_t* valid;
+    int32_t kind;
+    int32_t dtype;
+    int32_t word;    // offset of the state's first word inside the slot (key is word 0)
+    int32_t nwords;
+};
+
+struct PredDesc {
+    const void* col;
+    const uint8_t* valid;
+    int32_t dtype;
+    int32_t cmp;
+    ll lit_i;
+    double lit_f;
+};
+
+struct AggOut {
+    int32_t op;
+    int32_t in_dtype;
+    int32_t out_dtype;
+    int32_t sum_state;   // index into states or -1
+    int32_t cnt_state;   // state deciding NULL-ness / COUNT value, or -1
+    int32_t mm_state;    // MIN/MAX state or -1
+    int32_t nullable;    // output can be NULL (input column has validity)
+    int32_t pad;
+    void* out;
+    uint8_t* out_valid;
+};
+
+struct GbParams {
+    const void* kcol[2];
+    const uint8_t* kvalid[2];
+    int32_t kdtype[2];
+    int32_t n_keys;
+    int32_t n_pred;
+    PredDesc pred[GB_MAX_PREDS];
+    StateDesc st[GB_MAX_STATES];
+    int32_t n_st;
+    int32_t slot_words;
+    uint64_t row_begin;
+    uint64_t n_rows;
+    ull* gtab;           // (cap + 2) * slot_words words; slot cap = key -1, cap + 1 = NULL key
+    int32_t log2cap;
+    uint32_t max_probe;
+    int32_t smem_log2;   // 0 disables the shared-memory tier
+    int32_t fx_e;
+    int32_t warp_agg;
+    uint32_t* status;
+    ull* occupancy;
+    ull grow_limit;
+};
+
+struct GbFinal {
+    ull* gtab;
+    int32_t slot_words;
+    int32_t log2cap;
+    int32_t n_keys;
+    int32_t kdtype[2];
+    int32_t n_aggs;
+    int32_t fx_e;
+    StateDesc st[GB_MAX_STATES];
+    AggOut agg[GB_MAX_AGGS];
+    void* out_key[2];
+    uint8_t* out_key_valid[2];
+    uint64_t out_cap;
+    ull* order_keys;     // compacted order keys (large path)
+    uint32_t* slots;     // compacted slots
+    uint32_t* sorted;    // sorted slots
+    ull* n_nonnull;      // device: groups excluding the NULL group
+    ull* n_groups;       // device: groups written (incl. NULL group)
+    ull* n_groups_user;  // optional user device word
+    uint32_t* status;
+};
+
+// A fully planned GROUP BY (one query).
+struct GbPlan {
+    GbParams prm;
+    GbFinal fin;
+    uint64_t cap = 0;
+    int32_t smem_entries = 0;
+    int32_t block = 512;
+    int32_t grid = 0;
+    int32_t u = 4;
+    int32_t n_aggs = 0;
+    bool small_final = false;
+    int32_t mode = 0;
+    uint32_t flags = 0;
+};
+
+// Plan modes selected after a flagged first attempt.
+constexpr int GB_MODE_F64_ATOMIC = 1;  // f64 SUM with plain atomics (non-finite / huge inputs)
+constexpr int GB_MODE_WIDE_DEC = 2;    // Decimal128 SUM with the exact 192-bit state
+
+// Builds the plan for `desc` over rows [row_begin, row_end) (no device work).
+bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* desc, const bolt_groupby_out* out,
+                    uint64_t row_begin, uint64_t row_end, uint32_t flags, int mode,
+                    uint64_t cap_override, GbPlan* plan);
+
+// Bytes of scratch the plan needs (table + finalize buffers).
+uint64_t gb_plan_scratch(const GbPlan& plan);
+
+// Allocates scratch and enqueues table init, aggregation and finalize.
+bolt_status gb_enqueue(bolt_ctx* ctx, GbPlan* plan, cudaStream_t s);
+
+}  // namespace bolt

@@ -1,0 +1,91 @@
+"""CPU: the C-ABI library loads, exports every entry point the header
+declares, its struct layouts match the ctypes binding, and calls without a
+GPU fail with a typed status (no crash) — the reference's cuda-stub contract
+(tests/cuda_stub_contract_test.rs:1-20)."""
+
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+import tempfile
+from pathlib import Path
+
+import pytest
+
+from conftest import REPO, gpu_available, load_bolt
+
+HEADER = REPO / "include" / "bolt_b200.h"
+
+
+def header_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bolt_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    bolt = load_bolt()
+    from importlib import import_module
+    build = import_module("craton_bolt_b200.build")
+    build.build()
+    return bolt.lib()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = header_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_binding_covers_every_declared_function():
+    from importlib import import_module
+    load_bolt()
+    abi = import_module("craton_bolt_b200._abi")
+    assert sorted(abi.SIGNATURES) == header_functions()
+
+
+def test_struct_layouts_match_header(tmp_path):
+    from importlib import import_module
+    load_bolt()
+    abi = import_module("craton_bolt_b200._abi")
+    structs = {"bolt_col_view": abi.ColView, "bolt_col_mut": abi.ColMut, "bolt_agg_spec": abi.AggSpec,
+               "bolt_pred": abi.Pred, "bolt_groupby_desc": abi.GroupbyDesc, "bolt_groupby_out": abi.GroupbyOut,
+               "bolt_query": abi.Query, "bolt_server_config": abi.ServerConfig}
+    src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){"]
+    for cname, py in structs.items():
+        src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            src.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    src.append("return 0;}")
+    c_file = tmp_path / "layout.c"
+    c_file.write_text("\n".join(src))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-o", str(exe), str(c_file)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = dict(line.rsplit(" ", 1) for line in out if line)
+    for cname, py in structs.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, f"{cname}.{fname}"
+
+
+def test_status_strings(lib):
+    lib.bolt_status_str.restype = C.c_char_p
+    assert lib.bolt_status_str(0) == b"ok"
+    assert lib.bolt_status_str(3) == b"overflow"
+    assert lib.bolt_version().startswith(b"bolt-b200")
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU contract")
+def test_no_gpu_gives_typed_error(lib):
+    h = C.c_void_p()
+    st = lib.bolt_ctx_create(0, 0, C.byref(h))
+    assert st == 6 and not h.value  # BOLT_ERR_CUDA, no context
+
+
+def test_null_context_is_rejected(lib):
+    assert lib.bolt_groupby(None, None, None, 0, None) == 7
+    assert lib.bolt_radix_sort_perm(None, None, 0, 0, None, 0, None) == 7

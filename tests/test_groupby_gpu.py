@@ -1,0 +1,227 @@
+"""GPU parity: bolt_groupby (through the C ABI) against the CPU oracle."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import (REL_TOL, assert_float_close, bitmap, compare_groupby, golden, spec_arrays,
+                     split_packed, unpack_bits)
+
+pytestmark = pytest.mark.gpu
+
+
+def tables(bolt, oracle, cols: dict):
+    """numpy columns {name: (data, validity bitmap|None, dtype, scale)} ->
+    (device Columns, oracle HostCols)."""
+    dev, host = {}, {}
+    for name, (data, valid, dt, scale) in cols.items():
+        c = bolt.col(data, dt, valid, scale)
+        dev[name] = c.to("cuda")
+        host[name] = oracle.HostCol(data, dt, valid, scale)
+    return dev, host
+
+
+def run_both(bolt, engine, oracle, cols, group_by, aggs, where=(), hint=0, flags=0, rel=REL_TOL):
+    dev, host = tables(bolt, oracle, cols)
+    res = engine.execute_groupby(dev, group_by, aggs, where=where, groups_hint=hint, flags=flags)
+    orc = oracle.groupby(host, group_by, aggs, where=where)
+    in_dts = [cols[c][2] if c is not None else None for _, c in aggs]
+    compare_groupby(res, orc, [cols[k][2] for k in group_by], aggs, in_dts, rel)
+    return res, orc
+
+
+@pytest.mark.parametrize("case", [c for c in golden()["groupby"] if "error" not in c["expected"]],
+                         ids=lambda c: c["name"])
+def test_groupby_known_answers(bolt, engine, oracle, case):
+    cols = {k: spec_arrays(v) for k, v in case["columns"].items()}
+    aggs = [tuple(a) for a in case["aggs"]]
+    run_both(bolt, engine, oracle, cols, case["group_by"], aggs)
+
+
+def test_groupby_decimal_overflow_known_answer(bolt, engine, oracle):
+    case = [c for c in golden()["groupby"] if c["name"] == "decimal_sum_overflow"][0]
+    cols = {k: spec_arrays(v) for k, v in case["columns"].items()}
+    dev, _ = tables(bolt, oracle, cols)
+    with pytest.raises(bolt.TypeError_) as ei:
+        engine.execute_groupby(dev, ["k"], [("sum", "d")])
+    assert "overflow" in str(ei.value) and "Decimal128" in str(ei.value)
+
+
+def small_config(n, seed=1):
+    import importlib
+    dg = importlib.import_module("craton_bolt_b200.datagen")
+    d = dg.groupby_small(n, seed)
+    return {"k": (d["k"], None, "i32", 0), "v": (d["v"], None, "i64", 0)}
+
+
+@pytest.mark.parametrize("flags_name", ["default", "force_global"])
+def test_groupby_plain_single_key(bolt, engine, oracle, flags_name):
+    """SELECT k, SUM(v), COUNT(*), MIN(v), MAX(v) GROUP BY k on 1,000,000 rows."""
+    flags = bolt.FLAG_FORCE_GLOBAL if flags_name == "force_global" else 0
+    cols = small_config(1_000_000)
+    aggs = [("sum", "v"), ("count_star", None), ("min", "v"), ("max", "v")]
+    res, orc = run_both(bolt, engine, oracle, cols, ["k"], aggs, hint=1024, flags=flags)
+    assert res.n_groups == 1024
+
+
+def test_groupby_plain_no_hint_grows(bolt, engine, oracle):
+    cols = small_config(300_000, seed=5)
+    aggs = [("sum", "v"), ("count_star", None)]
+    run_both(bolt, engine, oracle, cols, ["k"], aggs, hint=0)
+
+
+def filtered_config(n, n_pairs, seed=2):
+    import importlib
+    dg = importlib.import_module("craton_bolt_b200.datagen")
+    d = dg.groupby_filtered(n, seed, n_pairs=n_pairs)
+    return {"a": (d["a"], None, "i32", 0), "b": (d["b"], None, "i32", 0), "f": (d["f"], None, "i32", 0),
+            "vd": (d["vd"], None, "f64", 0), "vi": (d["vi"], None, "i64", 0)}
+
+
+FILTERED_AGGS = [("sum", "vd"), ("avg", "vd"), ("count_star", None), ("min", "vi"), ("max", "vi")]
+
+
+@pytest.mark.parametrize("n,n_pairs,hint", [(200_000, 50_000, 0), (2_000_000, 1_000_000, 400_000),
+                                            (3_000_000, 10_000_000, 0)])
+def test_groupby_filtered_two_key(bolt, engine, oracle, n, n_pairs, hint):
+    """Filtered high-cardinality two-key GROUP BY (Zipf pairs, f < 50)."""
+    cols = filtered_config(n, n_pairs)
+    res, orc = run_both(bolt, engine, oracle, cols, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)], hint=hint)
+    assert res.n_groups > 1000
+
+
+def test_groupby_f64_sum_is_order_independent(bolt, engine, oracle):
+    """Fixed-point f64 sums: bit-identical across runs and table tiers."""
+    cols = filtered_config(500_000, 20_000, seed=7)
+    dev, _ = tables(bolt, oracle, cols)
+    r1 = engine.execute_groupby(dev, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)])
+    r2 = engine.execute_groupby(dev, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)], flags=bolt.FLAG_FORCE_GLOBAL)
+    for x, y in zip(r1.aggs, r2.aggs):
+        assert torch.equal(x.data.view(torch.int64) if x.dtype == "f64" else x.data,
+                           y.data.view(torch.int64) if y.dtype == "f64" else y.data)
+
+
+def test_groupby_f64_sum_close_to_exact(bolt, engine, oracle):
+    """The fixed-point SUM is within one ulp of the compensated (accurate) sum."""
+    cols = filtered_config(400_000, 5_000, seed=11)
+    dev, host = tables(bolt, oracle, cols)
+    res = engine.execute_groupby(dev, ["a", "b"], [("sum", "vd")], where=[("f", "<", 50)])
+    orc = oracle.groupby(host, ["a", "b"], [("sum", "vd")], where=[("f", "<", 50)])
+    got = res.aggs[0].numpy()
+    acc = orc["accurate"][0]
+    ulp = np.spacing(np.abs(acc))
+    assert np.all(np.abs(got - acc) <= ulp + 1e-15)
+
+
+def test_groupby_null_keys_and_values(bolt, engine, oracle):
+    rng = np.random.default_rng(3)
+    n = 100_000
+    k = rng.integers(-500, 500, n).astype(np.int32)
+    kv = rng.random(n) > 0.02
+    v = rng.integers(-2**40, 2**40, n).astype(np.int64)
+    vv = rng.random(n) > 0.3
+    d = rng.normal(0, 5, n)
+    dv = rng.random(n) > 0.5
+    cols = {"k": (k, bitmap(kv), "i32", 0), "v": (v, bitmap(vv), "i64", 0), "d": (d, bitmap(dv), "f64", 0)}
+    aggs = [("count_star", None), ("count", "v"), ("sum", "v"), ("min", "v"), ("max", "v"), ("avg", "d"),
+            ("min", "d")]
+    run_both(bolt, engine, oracle, cols, ["k"], aggs)
+
+
+def test_groupby_key_dtypes(bolt, engine, oracle):
+    rng = np.random.default_rng(4)
+    n = 50_000
+    base = rng.integers(0, 300, n)
+    cases = {
+        "i64": (base.astype(np.int64) * 1_000_000_007 - 2**62, "i64"),
+        "f64": (np.where(base % 7 == 0, -0.0, base / 3.0 - 20.0), "f64"),
+        "f32": (np.where(base % 5 == 0, np.float32(np.nan), (base / 7.0).astype(np.float32)).astype(np.float32), "f32"),
+    }
+    for name, (kd, dt) in cases.items():
+        cols = {"k": (kd, None, dt, 0), "v": (base.astype(np.int32), None, "i32", 0)}
+        run_both(bolt, engine, oracle, cols, ["k"], [("sum", "v"), ("count_star", None), ("max", "v")])
+
+
+def test_groupby_sentinel_key_minus_one(bolt, engine, oracle):
+    """Key -1 packs to all ones (the value whose complement marks empty slots)."""
+    k = np.array([-1, 5, -1, 7, -1, 5], np.int32)
+    v = np.arange(6, dtype=np.int64)
+    run_both(bolt, engine, oracle, {"k": (k, None, "i32", 0), "v": (v, None, "i64", 0)}, ["k"],
+             [("sum", "v"), ("count_star", None)])
+    a = np.array([-1, -1, 0, -1], np.int32)
+    b = np.array([-1, -1, 0, 3], np.int32)
+    run_both(bolt, engine, oracle, {"a": (a, None, "i32", 0), "b": (b, None, "i32", 0)}, ["a", "b"],
+             [("count_star", None)])
+
+
+def test_groupby_sum_i64_overflow(bolt, engine, oracle):
+    k = np.zeros(4, np.int32)
+    v = np.array([2**62, 2**62, 5, 7], np.int64)
+    dev, _ = tables(bolt, oracle, {"k": (k, None, "i32", 0), "v": (v, None, "i64", 0)})
+    with pytest.raises(bolt.TypeError_) as ei:
+        engine.execute_groupby(dev, ["k"], [("sum", "v")])
+    assert "SUM(integer) overflow" in str(ei.value)
+
+
+def test_groupby_empty_input_and_all_filtered(bolt, engine, oracle):
+    k = np.zeros(0, np.int32)
+    v = np.zeros(0, np.int64)
+    res, _ = run_both(bolt, engine, oracle, {"k": (k, None, "i32", 0), "v": (v, None, "i64", 0)}, ["k"],
+                      [("sum", "v")])
+    assert res.n_groups == 0
+    k = np.arange(1000, dtype=np.int32)
+    f = np.full(1000, 99, np.int32)
+    res, _ = run_both(bolt, engine, oracle, {"k": (k, None, "i32", 0), "f": (f, None, "i32", 0)}, ["k"],
+                      [("count_star", None)], where=[("f", "<", 50)])
+    assert res.n_groups == 0
+
+
+def test_groupby_single_hot_key(bolt, engine, oracle):
+    """Every row in one group (maximal atomic contention)."""
+    n = 2_000_000
+    k = np.full(n, 42, np.int32)
+    v = np.random.default_rng(8).integers(-1000, 1000, n).astype(np.int64)
+    d = np.random.default_rng(9).normal(0, 1e3, n)
+    run_both(bolt, engine, oracle, {"k": (k, None, "i32", 0), "v": (v, None, "i64", 0), "d": (d, None, "f64", 0)},
+             ["k"], [("sum", "v"), ("sum", "d"), ("count_star", None), ("min", "v"), ("max", "d")])
+
+
+def test_groupby_nonfinite_f64_falls_back(bolt, engine, oracle):
+    k = np.array([0, 0, 1, 1, 2, 2], np.int32)
+    d = np.array([1.0, np.inf, 2.0, 3.0, 1e300, 1e300], np.float64)
+    dev, host = tables(bolt, oracle, {"k": (k, None, "i32", 0), "d": (d, None, "f64", 0)})
+    res = engine.execute_groupby(dev, ["k"], [("sum", "d")])
+    got = res.aggs[0].numpy()
+    assert got[0] == np.inf and got[1] == 5.0 and got[2] == 2e300
+
+
+def test_groupby_where_float_and_multiple_conjuncts(bolt, engine, oracle):
+    rng = np.random.default_rng(12)
+    n = 200_000
+    cols = {"k": (rng.integers(0, 2000, n).astype(np.int32), None, "i32", 0),
+            "x": (rng.normal(0, 1, n), None, "f64", 0),
+            "y": (rng.integers(-100, 100, n).astype(np.int64), None, "i64", 0)}
+    run_both(bolt, engine, oracle, cols, ["k"], [("sum", "y"), ("avg", "x"), ("count_star", None)],
+             where=[("x", ">", 0.25), ("y", "!=", 3), ("y", ">=", -50)])
+
+
+def test_groupby_decline_unsupported(bolt, engine, oracle):
+    k = np.zeros(4, np.int64)
+    v = np.zeros(4, np.int64)
+    dev, _ = tables(bolt, oracle, {"a": (k, None, "i64", 0), "b": (v, None, "i64", 0)})
+    assert engine.try_execute_groupby(dev, ["a", "b"], [("count_star", None)]) is None
+
+
+def test_groupby_host_inputs_end_to_end(bolt, engine, oracle):
+    """Host numpy columns in, host columns out (the end-to-end path)."""
+    cols = small_config(100_000, seed=9)
+    host = {k: bolt.col(v[0], v[2]) for k, v in cols.items()}
+    res = engine.execute_groupby(host, ["k"], [("sum", "v"), ("count_star", None)], groups_hint=1024)
+    assert not res.keys[0].is_cuda
+    orc = oracle.groupby({k: oracle.HostCol(v[0], v[2]) for k, v in cols.items()}, ["k"],
+                         [("sum", "v"), ("count_star", None)])
+    compare_groupby(res, orc, ["i32"], [("sum", "v"), ("count_star", None)], ["i64", None])

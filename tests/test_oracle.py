@@ -1,0 +1,231 @@
+"""CPU: the oracle against the reference's known answers and an independent
+pure-Python restatement on small seeded inputs."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from helpers import golden, spec_arrays, split_packed, unpack_bits
+
+
+def host_table(oracle, columns: dict) -> dict:
+    out = {}
+    for name, spec in columns.items():
+        data, valid, dt, scale = spec_arrays(spec)
+        out[name] = oracle.HostCol(data, dt, valid, scale)
+    return out
+
+
+def _eq(a, b) -> bool:
+    if isinstance(b, float) or isinstance(a, float):
+        a, b = float(a), float(b)
+        return (math.isnan(a) and math.isnan(b)) or a == b
+    return int(a) == int(b)
+
+
+@pytest.mark.parametrize("case", golden()["groupby"], ids=lambda c: c["name"])
+def test_oracle_groupby_known_answers(oracle, case):
+    t = host_table(oracle, case["columns"])
+    exp = case["expected"]
+    aggs = [tuple(a) for a in case["aggs"]]
+    if "error" in exp:
+        with pytest.raises(oracle.OracleError) as ei:
+            oracle.groupby(t, case["group_by"], aggs)
+        assert ei.value.status == oracle.OVERFLOW
+        for word in exp["message_contains"]:
+            assert word in str(ei.value)
+        return
+    r = oracle.groupby(t, case["group_by"], aggs)
+    assert r["n_groups"] == len(exp["keys"])
+    dts = [case["columns"][k]["dtype"] for k in case["group_by"]]
+    keys = split_packed(r["keys"], dts)
+    for g, want in enumerate(exp["keys"]):
+        if want == [None]:
+            assert r["key_null"][g]
+            continue
+        assert not r["key_null"][g]
+        assert [int(k[g]) for k in keys] == want
+    for a, (vals, valid) in enumerate(zip(exp["aggs"], exp["agg_valid"])):
+        for g in range(len(vals)):
+            assert bool(r["valid"][a][g]) == bool(valid[g]), (case["name"], a, g)
+            if not valid[g]:
+                continue
+            got = r["vals"][a][g]
+            if case["columns"].get(aggs[a][1] or "", {}).get("dtype") == "dec128":
+                lo, hi = int(got[0]) & (2**64 - 1), int(got[1])
+                got = (hi << 64) | lo
+            want = vals[g]
+            if want == "NaN":
+                want = math.nan
+            assert _eq(got, want), (case["name"], a, g, got, want)
+
+
+@pytest.mark.parametrize("case", golden()["join"], ids=lambda c: c["name"])
+def test_oracle_join_known_answers(oracle, case):
+    bd, bv, bdt, _ = spec_arrays(case["build"])
+    pd, pv, pdt, _ = spec_arrays(case["probe"])
+    b = oracle.HostCol(bd, bdt, bv)
+    p = oracle.HostCol(pd, pdt, pv)
+    pr, br = oracle.hash_join(b, p)
+    assert len(pr) == case["expected"]["n_pairs"]
+    if len(pr):
+        pk = spec_arrays(case["probe"])[0]
+        bk = spec_arrays(case["build"])[0]
+        assert np.array_equal(bk[br], pk[pr])
+        assert np.all(np.diff(pr.astype(np.int64)) > 0)  # probe order
+
+
+@pytest.mark.parametrize("case", golden()["sort_keys"], ids=lambda c: c["name"])
+def test_oracle_sort_key_transform(oracle, case):
+    dt = case["dtype"]
+    if "bits" in case:
+        data = np.array(case["bits"], dtype=np.uint32).view(np.float32)
+    else:
+        data = np.array([float(v) for v in case["values"]], dtype=np.float32 if dt == "f32" else np.float64)
+    k = oracle.sort_keys(oracle.HostCol(data, dt), case.get("descending", False)).astype(np.uint64)
+    prop = case["property"]
+    if prop == "strictly_increasing":
+        assert np.all(np.diff(k.astype(object)) > 0)
+    elif prop == "strictly_decreasing":
+        assert np.all(np.diff(k.astype(object)) < 0)
+    elif prop == "all_equal":
+        assert len(set(k.tolist())) == 1
+    else:
+        assert len(set(k.tolist())) == 1
+        inf = oracle.sort_keys(oracle.HostCol(np.array([np.inf], np.float32), "f32"))[0]
+        assert int(k[0]) > int(inf)
+
+
+def sort_input(oracle, case):
+    n = case["n"]
+    if case["gen"] == "shuffle_iota":
+        v = oracle.shuffle_deterministic(np.arange(n, dtype=np.uint32), case["seed"]).view(np.int32)
+        return v.astype(np.int32)
+    if case["gen"] == "mul7919_mod_shuffle":
+        base = (np.arange(n, dtype=np.int64) * 7919) % 1_000_000
+        idx = oracle.shuffle_deterministic(np.arange(n, dtype=np.uint32), case["seed"]).astype(np.int64)
+        return base[idx]
+    return np.sin(np.arange(n, dtype=np.float64) * 1.61803398875)
+
+
+@pytest.mark.parametrize("case", golden()["sort"], ids=lambda c: c["name"])
+def test_oracle_sort_known_answers(oracle, case):
+    v = sort_input(oracle, case)
+    perm = oracle.sort_perm(oracle.HostCol(v, case["dtype"]), case["descending"])
+    out = v[perm]
+    want = np.sort(v)[::-1] if case["descending"] else np.sort(v)
+    assert np.array_equal(out, want)
+    # stability: equal keys keep input order
+    same = out[1:] == out[:-1]
+    assert np.all(perm[1:][same] > perm[:-1][same])
+
+
+def test_shuffle_deterministic_is_a_permutation(oracle):
+    a = oracle.shuffle_deterministic(np.arange(1000, dtype=np.uint32), 7)
+    assert sorted(a.tolist()) == list(range(1000))
+    assert not np.array_equal(a, np.arange(1000))
+
+
+def test_xorshift64star_matches_python_restatement(oracle):
+    seed = 0xB2
+    s = (seed + 0x9E3779B97F4A7C15) & (2**64 - 1)
+    want = []
+    for _ in range(64):
+        s ^= s >> 12
+        s ^= (s << 25) & (2**64 - 1)
+        s ^= s >> 27
+        want.append((s * 0x2545F4914F6CDD1D) & (2**64 - 1))
+    assert oracle.xorshift64star(seed, 64).tolist() == want
+
+
+# ---------------------------------------------------------------------------
+# Independent pure-Python restatement (small sizes only)
+# ---------------------------------------------------------------------------
+def py_groupby(k, kvalid, v, vvalid, f, lit):
+    groups = {}
+    for i in range(len(k)):
+        if not (f[i] < lit):
+            continue
+        key = None if not kvalid[i] else int(k[i])
+        g = groups.setdefault(key, {"cnt": 0, "n": 0, "sum": 0, "min": None, "max": None, "fsum": 0.0})
+        g["cnt"] += 1
+        if vvalid[i]:
+            x = int(v[i])
+            g["n"] += 1
+            g["sum"] += x
+            g["fsum"] += float(x)
+            g["min"] = x if g["min"] is None else min(g["min"], x)
+            g["max"] = x if g["max"] is None else max(g["max"], x)
+    order = sorted([kk for kk in groups if kk is not None]) + ([None] if None in groups else [])
+    return order, groups
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_groupby_matches_python(oracle, seed):
+    rng = np.random.default_rng(seed)
+    n = 3000
+    k = rng.integers(-50, 50, n).astype(np.int32)
+    kvalid = rng.random(n) > 0.05
+    v = rng.integers(-10**6, 10**6, n).astype(np.int64)
+    vvalid = rng.random(n) > 0.1
+    f = rng.integers(0, 100, n).astype(np.int32)
+    bm = lambda m: np.packbits(m.astype(np.uint8), bitorder="little")
+    t = {"k": oracle.HostCol(k, "i32", bm(kvalid)), "v": oracle.HostCol(v, "i64", bm(vvalid)),
+         "f": oracle.HostCol(f, "i32")}
+    aggs = [("count_star", None), ("count", "v"), ("sum", "v"), ("min", "v"), ("max", "v"), ("avg", "v")]
+    r = oracle.groupby(t, ["k"], aggs, where=[("f", "<", 50)])
+    order, groups = py_groupby(k, kvalid, v, vvalid, f, 50)
+    assert r["n_groups"] == len(order)
+    for gi, key in enumerate(order):
+        g = groups[key]
+        assert r["key_null"][gi] == (key is None)
+        if key is not None:
+            assert int(r["keys"][gi]) == key
+        assert r["vals"][0][gi] == g["cnt"]
+        assert r["vals"][1][gi] == g["n"]
+        assert bool(r["valid"][2][gi]) == (g["n"] > 0)
+        if g["n"]:
+            assert r["vals"][2][gi] == g["sum"]
+            assert r["vals"][3][gi] == g["min"]
+            assert r["vals"][4][gi] == g["max"]
+            assert r["vals"][5][gi] == g["fsum"] / g["n"]
+
+
+def test_oracle_two_key_packing_and_order(oracle):
+    a = np.array([1, -1, 1, 0, -1], np.int32)
+    b = np.array([-1, 5, 2, 7, 5], np.int32)
+    t = {"a": oracle.HostCol(a, "i32"), "b": oracle.HostCol(b, "i32")}
+    r = oracle.groupby(t, ["a", "b"], [("count_star", None)])
+    packed = [((int(x) & 0xFFFFFFFF) << 32 | (int(y) & 0xFFFFFFFF)) for x, y in zip(a, b)]
+    packed = [p - (1 << 64) if p >= (1 << 63) else p for p in packed]
+    assert r["keys"].tolist() == sorted(set(packed))
+    assert r["vals"][0].tolist() == [2, 1, 1, 1]
+
+
+def test_oracle_sum_i64_overflow_message(oracle):
+    t = {"k": oracle.HostCol(np.zeros(2, np.int32), "i32"),
+         "v": oracle.HostCol(np.array([2**62, 2**62], np.int64), "i64")}
+    with pytest.raises(oracle.OracleError) as ei:
+        oracle.groupby(t, ["k"], [("sum", "v")])
+    assert "SUM(integer) overflow" in str(ei.value)
+
+
+def test_oracle_compact_order(oracle):
+    rng = np.random.default_rng(9)
+    f = rng.integers(0, 100, 5000).astype(np.int32)
+    rows = oracle.compact({"f": oracle.HostCol(f, "i32")}, [("f", "<", 50)])
+    assert np.array_equal(rows, np.flatnonzero(f < 50).astype(np.uint32))
+
+
+def test_oracle_sort_nulls_last_and_first(oracle):
+    v = np.array([3, 1, 2, 1, 0], np.int32)
+    valid = np.array([1, 0, 1, 1, 0], bool)
+    bm = np.packbits(valid.astype(np.uint8), bitorder="little")
+    last = oracle.sort_perm(oracle.HostCol(v, "i32", bm), False, False)
+    first = oracle.sort_perm(oracle.HostCol(v, "i32", bm), False, True)
+    assert last.tolist() == [3, 2, 0, 1, 4]
+    assert first.tolist() == [1, 4, 3, 2, 0]
+    assert unpack_bits(bm, 5).tolist() == valid.tolist()
