@@ -1,32 +1,42 @@
 #!/usr/bin/env python
 """Benchmark of the B200 relational hot path (one JSON line on rank 0).
 
-Default workload: the filtered high-cardinality two-key GROUP BY
+Default workload (`--workload groupby_filtered`): the filtered
+high-cardinality two-key GROUP BY
   SELECT a, b, SUM(vd), AVG(vd), COUNT(*), MIN(vi), MAX(vi)
   FROM t WHERE f < 50 GROUP BY a, b
 over 100,000,000 seeded synthetic rows ((a, b) int32 pairs of 10M Zipf(1.1)
 ranks, f int32 U[0,100), vd f64 N(0,1e3), vi int64 uniform).
 
-  value      rows/s with the columns resident in HBM (device-timed, K steps)
-  e2e        rows/s through the public API from pinned host columns,
-             host->device copies and result readback inside the timed region
-  roofline   the aggregation kernel's algorithmic bytes / its CUDA-event time
-  cpu_baseline  the CPU oracle (restatement of the reference's host path)
+Other workloads (per-operator lines): groupby_plain (1M rows, 1024 keys),
+join_groupby (10M-row build, 200M-row probe, Decimal128 SUM), sort_i64
+(256M int64 keys), sort_f32 (64M float32 keys with specials), compact
+(100M-row WHERE compaction), batch (4096 filter + GROUP BY queries,
+batched / served vs one at a time).
+
+  value      rows/s (queries/s for batch) with inputs resident in HBM,
+             device-timed over K steps (CUDA events on the launch stream)
+  e2e        the same metric through the public API from pinned host
+             columns, host->device copies and result readback timed
+  roofline   the dominant kernel's algorithmic bytes / its CUDA-event time
+  cpu_baseline  the CPU restatement of the reference's host path (oracle)
              on a bounded sample of the same rows
 
 `--impl reference` times the CPU restatement of the reference's host path
-(the reference itself is Rust and cannot be built here) on the same
-workload and prints the same line with "impl": "reference".
-Multi-GPU (torchrun): independent replicas, one per rank; value sums all
-ranks' rows over the max per-rank device time.
+(the reference itself is Rust and cannot be built here) on the workload and
+prints the same line with "impl": "reference". Multi-GPU (torchrun): the
+path is run as independent replicas, one per rank; value sums all ranks'
+rows over the max per-rank device time.
 """
 
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import importlib
 import importlib.util
 import json
+import math
 import os
 import statistics
 import sys
@@ -50,6 +60,20 @@ def load_package():
     sys.modules[name] = mod
     spec.loader.exec_module(mod)
     return mod
+
+
+def datagen():
+    load_package()
+    return importlib.import_module("craton_bolt_b200.datagen")
+
+
+def oracle_mod():
+    if str(REPO) not in sys.path:
+        sys.path.insert(0, str(REPO))
+    import oracle
+
+    oracle.build()
+    return oracle
 
 
 def measured_peak_gbs():
@@ -122,7 +146,6 @@ class ClockSampler:
             note = "timed region shorter than the sampling period: warm-up and timed samples"
         nv = self.nv
         names = {
-            "gpu_idle": getattr(nv, "nvmlClocksEventReasonGpuIdle", 0x1),
             "applications_clocks_setting": getattr(nv, "nvmlClocksEventReasonApplicationsClocksSetting", 0x2),
             "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
             "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
@@ -134,7 +157,7 @@ class ClockSampler:
         reasons = set()
         for _, _, rs in inside:
             for k, bit in names.items():
-                if rs & bit and k != "gpu_idle":
+                if rs & bit:
                     reasons.add(k)
         mhz = [s[1] for s in inside]
         return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": self.max_mhz,
@@ -142,16 +165,131 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# Workload: filtered two-key GROUP BY
+# Shared timing harness
+# ---------------------------------------------------------------------------
+class Ctx:
+    """Per-rank state shared by the workloads."""
+
+    def __init__(self, args):
+        import torch
+
+        self.args = args
+        self.torch = torch
+        self.rank = int(os.environ.get("RANK", 0))
+        self.world = int(os.environ.get("WORLD_SIZE", 1))
+        self.local = int(os.environ.get("LOCAL_RANK", 0))
+        torch.cuda.set_device(self.local)
+        self.dev = f"cuda:{self.local}"
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.dist = dist
+        self.bolt = load_package()
+        self.eng = self.bolt.Engine(self.local, scratch_bytes=args.scratch_gb << 30)
+        self.lib = self.eng._lib
+        self.stream = torch.cuda.current_stream(self.local)
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max_over_ranks(self, v: float) -> float:
+        if not self.dist:
+            return v
+        t = self.torch.tensor([v], device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def check(self, what: str):
+        st = self.lib.bolt_ctx_sync_status(self.eng._ctx, self.stream.cuda_stream)
+        if st != 0:
+            raise RuntimeError(f"{what}: status {st}: {self.lib.bolt_ctx_last_error(self.eng._ctx).decode()}")
+
+    def kernel_times(self, last: int):
+        kt = (C.c_double * 4096)()
+        nk = self.lib.bolt_ctx_kernel_times(self.eng._ctx, kt, 4096)
+        return [kt[i] for i in range(nk)][-last:]
+
+    def timed(self, step, steps: int, warmup: int):
+        """Runs warmup + K async steps; returns (device ms, launches, kernel ms list, clocks)."""
+        torch = self.torch
+        sampler = ClockSampler(self.local)
+        sampler.start()
+        for _ in range(warmup):
+            step()
+        self.check("warm-up")
+        self.kernel_times(4096)
+        self.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches = 0
+        t0 = time.perf_counter()
+        e0.record(self.stream)
+        for _ in range(steps):
+            launches += step()
+        e1.record(self.stream)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        self.barrier()
+        ms = self.max_over_ranks(e0.elapsed_time(e1))
+        self.check("timed region")
+        kms = self.kernel_times(steps)
+        sampler.stop()
+        return ms, launches, kms, sampler.summary(t0, t1)
+
+    def time_e2e(self, step, steps: int) -> float:
+        torch = self.torch
+        step()
+        torch.cuda.synchronize()
+        self.barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(self.stream)
+        for _ in range(steps):
+            step()
+        f1.record(self.stream)
+        torch.cuda.synchronize()
+        return self.max_over_ranks(f0.elapsed_time(f1) / steps)
+
+
+def base_line(c: Ctx, ms: float, rows_per_step: float, alg_bytes: float, kms, kernel: str, workload: str,
+              config: dict, launches: int, clocks, dtype: str, unit: str = "rows/s"):
+    a = c.args
+    peak, peak_kind = measured_peak_gbs()
+    kern_ms = statistics.mean(kms) if kms else None
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9 if kern_ms else None
+    step_ms = ms / a.steps
+    return {
+        "metric": METRIC, "value": c.world * rows_per_step * a.steps / (ms * 1e-3), "unit": unit,
+        "n_gpus": c.world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "data": "synthetic (seeded splitmix64 generator; no dataset)",
+        "config": dict(config, parallelism=f"replicas x{c.world}" if c.world > 1 else "1 GPU"),
+        "hbm_gbs_step": alg_bytes / (step_ms * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": profiled_traffic(workload),
+                     "kernel": kernel, "kernel_ms": kern_ms, "algorithmic_bytes_per_launch": alg_bytes,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+
+
+# ---------------------------------------------------------------------------
+# Workload: filtered two-key GROUP BY (default)
 # ---------------------------------------------------------------------------
 FILTERED_AGGS = [("sum", "vd"), ("avg", "vd"), ("count_star", None), ("min", "vi"), ("max", "vi")]
 FILTERED_DT = {"a": "i32", "b": "i32", "f": "i32", "vd": "f64", "vi": "i64"}
-BYTES_PER_ROW = 4 + 4 + 4 + 8 + 8
+FILTERED_BYTES = 4 + 4 + 4 + 8 + 8
 
 
 def gen_filtered(n: int, device: str | None):
-    load_package()
-    dg = importlib.import_module("craton_bolt_b200.datagen")
+    dg = datagen()
     cdf = dg.zipf_cdf(10_000_000, 1.1)
     if device is not None:
         ranks = dg.zipf_ranks_torch(cdf, 2, n, device)
@@ -160,66 +298,383 @@ def gen_filtered(n: int, device: str | None):
     return dg.groupby_filtered(n, seed=2, ranks=ranks)
 
 
-class GroupbyCall:
-    """Prebuilt C-ABI call of the filtered GROUP BY on device-resident columns."""
+class PreparedCall:
+    """A prepared GROUP BY run through bolt_groupby with BOLT_FLAG_ASYNC."""
 
-    def __init__(self, bolt, eng, dev_cols: dict, groups_hint: int, out_cap: int):
-        import ctypes as C
-        import torch
+    def __init__(self, c: Ctx, pq):
+        self.c, self.pq = c, pq
+        self.ng = c.torch.zeros(1, dtype=c.torch.int64, device=c.dev)
+        pq.out.n_groups_dev = self.ng.data_ptr()
 
-        abi = importlib.import_module("craton_bolt_b200._abi")
-        self.C, self.abi, self.eng, self.lib = C, abi, eng, bolt.lib()
-        names = list(dev_cols)
-        self.keep = [dev_cols]
-        self.views = (abi.ColView * len(names))(*[dev_cols[k].view() for k in names])
-        self.kidx = (C.c_int32 * 2)(names.index("a"), names.index("b"))
-        self.preds = (abi.Pred * 1)(abi.Pred(names.index("f"), abi.CMP_CODES["<"], 50, 0.0))
-        self.specs = (abi.AggSpec * len(FILTERED_AGGS))(
-            *[abi.AggSpec(abi.AGG_CODES[op], names.index(c) if c else -1) for op, c in FILTERED_AGGS])
-        self.desc = abi.GroupbyDesc(self.views, len(names), self.kidx, 2, self.preds, 1, self.specs,
-                                    len(FILTERED_AGGS), groups_hint)
-        dev = dev_cols["a"].data.device
-        self.outs = [torch.empty(out_cap, dtype=torch.int32, device=dev), torch.empty(out_cap, dtype=torch.int32, device=dev)]
-        self.aouts = [torch.empty(out_cap, dtype=t, device=dev) for t in
-                      (torch.float64, torch.float64, torch.int64, torch.int64, torch.int64)]
-        self.ng = torch.zeros(1, dtype=torch.int64, device=dev)
-        kd = [abi.I32, abi.I32]
-        ad = [abi.F64, abi.F64, abi.I64, abi.I64, abi.I64]
-        self.kmut = (abi.ColMut * 2)(*[abi.ColMut(t.data_ptr(), None, out_cap, d, 0) for t, d in zip(self.outs, kd)])
-        self.amut = (abi.ColMut * 5)(*[abi.ColMut(t.data_ptr(), None, out_cap, d, 0) for t, d in zip(self.aouts, ad)])
-        self.out = abi.GroupbyOut(self.kmut, self.amut, 0, self.ng.data_ptr())
-
-    def __call__(self, stream_handle: int, flags: int):
-        st = self.lib.bolt_groupby(self.eng._ctx, self.C.byref(self.desc), self.C.byref(self.out), flags,
-                                   self.C.c_void_p(stream_handle))
+    def __call__(self):
+        c = self.c
+        st = c.lib.bolt_groupby(c.eng._ctx, C.byref(self.pq.desc), C.byref(self.pq.out),
+                                c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE, C.c_void_p(c.stream.cuda_stream))
         if st != 0:
-            raise RuntimeError(f"bolt_groupby failed: {self.lib.bolt_ctx_last_error(self.eng._ctx).decode()}")
-        return int(self.lib.bolt_ctx_last_launches(self.eng._ctx))
+            raise RuntimeError(f"bolt_groupby: {c.lib.bolt_ctx_last_error(c.eng._ctx).decode()}")
+        return int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
 
 
-def cpu_sample_rows_per_s(data: dict, n_sample: int, threads: int = 1):
-    sys.path.insert(0, str(REPO))
-    import oracle
-
-    oracle.build()
-    oracle.lib().orc_set_threads(threads)
-    host = {k: oracle.HostCol(np.ascontiguousarray(v[:n_sample]), FILTERED_DT[k]) for k, v in data.items()}
+def cpu_rows_per_s_groupby(table_np: dict, dts: dict, group_by, aggs, where, n_sample: int):
+    orc = oracle_mod()
+    host = {k: orc.HostCol(np.ascontiguousarray(v[:n_sample]), dts[k]) for k, v in table_np.items()}
     t0 = time.perf_counter()
-    oracle.groupby(host, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)])
-    dt = time.perf_counter() - t0
-    return n_sample / dt, dt
+    orc.groupby(host, group_by, aggs, where=where)
+    return n_sample / (time.perf_counter() - t0)
 
 
+def w_groupby_filtered(c: Ctx):
+    a = c.args
+    torch = c.torch
+    data = gen_filtered(a.rows, c.dev)
+    host = {k: torch.from_numpy(v).pin_memory() for k, v in data.items()}
+    dev = {k: c.bolt.Column(host[k].to(c.dev), FILTERED_DT[k]) for k in data}
+    torch.cuda.synchronize()
+    pq = c.eng.prepare_groupby(dev, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], groups_hint=a.groups_hint,
+                               out_cap=max(2 * a.groups_hint, 1 << 20))
+    call = PreparedCall(c, pq)
+    ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
+    n_groups = int(call.ng.item())
+    alg = a.rows * FILTERED_BYTES
+    line = base_line(c, ms, a.rows, alg, kms, "gb_agg_kernel", "groupby_filtered",
+                     {"workload": "filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) ranks, "
+                                  "WHERE f < 50, SUM/AVG(vd f64), COUNT(*), MIN/MAX(vi i64)",
+                      "rows": a.rows, "groups": n_groups, "groups_hint": a.groups_hint,
+                      "l2": "inputs (2.8 GB) larger than L2 (126 MB); no flush needed"},
+                     launches, clocks, "int64/f64")
+    if a.e2e_steps > 0:
+        hcols = {k: c.bolt.Column(host[k], FILTERED_DT[k]) for k in data}
+        res = {}
+
+        def e2e():
+            res["r"] = c.eng.execute_groupby(hcols, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
+                                             groups_hint=a.groups_hint)
+
+        e_ms = c.time_e2e(e2e, a.e2e_steps)
+        line["e2e"] = {"value": c.world * a.rows / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": alg,
+                       "d2h_bytes_per_step": res["r"].n_groups * (4 + 4 + 8 * 5), "ms_per_step": e_ms,
+                       "path": "Engine.execute_groupby on pinned host columns (H2D + GROUP BY + D2H)"}
+    if c.world == 1 and not a.no_cpu:
+        ns = min(a.cpu_rows, a.rows)
+        rps = cpu_rows_per_s_groupby(data, FILTERED_DT, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], ns)
+        line["cpu_baseline"] = {"value": rps, "unit": "rows/s", "cores": 1, "kind": "port",
+                                "sample": f"first {ns} rows of the workload; CPU restatement of the reference's "
+                                          "host GROUP BY (oracle), 1 thread"}
+    return line
+
+
+# ---------------------------------------------------------------------------
+# Workload: plain single-key GROUP BY (1M rows)
+# ---------------------------------------------------------------------------
+PLAIN_AGGS = [("sum", "v"), ("count_star", None), ("min", "v"), ("max", "v")]
+PLAIN_DT = {"k": "i32", "v": "i64"}
+
+
+def w_groupby_plain(c: Ctx):
+    a = c.args
+    torch = c.torch
+    n = a.plain_rows
+    data = datagen().groupby_small(n, seed=1)
+    host = {k: torch.from_numpy(v).pin_memory() for k, v in data.items()}
+    dev = {k: c.bolt.Column(host[k].to(c.dev), PLAIN_DT[k]) for k in data}
+    pq = c.eng.prepare_groupby(dev, ["k"], PLAIN_AGGS, groups_hint=1024)
+    call = PreparedCall(c, pq)
+    ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
+    alg = n * 12
+    line = base_line(c, ms, n, alg, kms, "gb_agg_kernel", "groupby_plain",
+                     {"workload": "plain single-key GROUP BY: 1M rows, k int32 U[0,1024), v int64 U[-1e6,1e6]; "
+                                  "SUM, COUNT(*), MIN, MAX", "rows": n, "groups_hint": 1024,
+                      "l2": "12 MB input fits in L2: warm-L2 figure (launch-bound workload)"},
+                     launches, clocks, "int64")
+    hcols = {k: c.bolt.Column(host[k], PLAIN_DT[k]) for k in data}
+    e_ms = c.time_e2e(lambda: c.eng.execute_groupby(hcols, ["k"], PLAIN_AGGS, groups_hint=1024), a.e2e_steps or 3)
+    line["e2e"] = {"value": n / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": alg,
+                   "d2h_bytes_per_step": 1024 * (4 + 32), "ms_per_step": e_ms}
+    if not a.no_cpu:
+        rps = cpu_rows_per_s_groupby(data, PLAIN_DT, ["k"], PLAIN_AGGS, [], n)
+        line["cpu_baseline"] = {"value": rps, "unit": "rows/s", "cores": 1, "kind": "port",
+                                "sample": f"all {n} rows, oracle GROUP BY, 1 thread"}
+    return line
+
+
+# ---------------------------------------------------------------------------
+# Workload: hash join then aggregate
+# ---------------------------------------------------------------------------
+def w_join_groupby(c: Ctx):
+    a = c.args
+    torch = c.torch
+    dg = datagen()
+    nb, npr = a.build_rows, a.probe_rows
+    bt = dg.join_build(nb, seed=3)
+    chunks = [dg.join_probe(min(1 << 25, npr - s), nb, seed=3, start=s) for s in range(0, npr, 1 << 25)]
+    pt = {"fk": np.concatenate([x["fk"] for x in chunks]), "amount": np.concatenate([x["amount"] for x in chunks])}
+    del chunks
+    bk = c.bolt.Column(torch.from_numpy(bt["k"]).to(c.dev), "i64")
+    bg = c.bolt.Column(torch.from_numpy(bt["g"]).to(c.dev), "i32")
+    pk = c.bolt.Column(torch.from_numpy(pt["fk"]).to(c.dev), "i64")
+    am = c.bolt.Column(torch.from_numpy(pt["amount"]).to(c.dev), "dec128", scale=2)
+    abi = importlib.import_module("craton_bolt_b200._abi")
+    g = torch.empty(4096, dtype=torch.int32, device=c.dev)
+    s = torch.empty((4096, 2), dtype=torch.int64, device=c.dev)
+    cnt = torch.empty(4096, dtype=torch.int64, device=c.dev)
+    gm = abi.ColMut(g.data_ptr(), None, 4096, abi.I32, 0)
+    sm = abi.ColMut(s.data_ptr(), None, 4096, abi.DEC128, 2)
+    cm = abi.ColMut(cnt.data_ptr(), None, 4096, abi.I64, 0)
+    ng = C.c_uint64(0)
+    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE
+    bkv, bgv, pkv, amv = bk.view(), bg.view(), pk.view(), am.view()
+
+    def step():
+        t = C.c_void_p()
+        st = c.lib.bolt_hash_join_build(c.eng._ctx, C.byref(bkv), C.byref(bgv), flags,
+                                        C.c_void_p(c.stream.cuda_stream), C.byref(t))
+        if st != 0:
+            raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+        n_l = int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
+        st = c.lib.bolt_join_groupby(c.eng._ctx, t, C.byref(pkv), C.byref(amv), C.byref(gm), C.byref(sm),
+                                     C.byref(cm), C.byref(ng), flags, C.c_void_p(c.stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+        n_l += int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
+        c.lib.bolt_hash_join_release(c.eng._ctx, t)
+        return n_l
+
+    ms, launches, kms, clocks = c.timed(step, a.steps, a.warmup)
+    # kernel times alternate build, probe-aggregate: the probe side dominates
+    probe_k = kms[1::2] if len(kms) >= 2 else kms
+    alg_probe = npr * 24
+    alg = nb * 12 + npr * 24
+    line = base_line(c, ms, npr, alg_probe, probe_k, "gb_agg_kernel (join lookup source)", "join_groupby",
+                     {"workload": "hash inner join then aggregate: build 10M unique shuffled int64 keys + int32 g; "
+                                  "probe 200M int64 fk (90% match), Decimal128(15,2) amount; GROUP BY g SUM, COUNT(*)",
+                      "build_rows": nb, "probe_rows": npr, "algorithmic_bytes_step": alg,
+                      "l2": "inputs (4.9 GB) larger than L2"}, launches, clocks, "int64/dec128")
+    line["note"] = "value counts probe rows per second; one step = build + fused probe/aggregate"
+    if not a.no_cpu:
+        orc = oracle_mod()
+        ns = min(a.cpu_rows, npr)
+        t0 = time.perf_counter()
+        orc.join_groupby(orc.HostCol(bt["k"], "i64"), bt["g"], orc.HostCol(pt["fk"][:ns], "i64"),
+                         orc.HostCol(pt["amount"][:ns], "dec128", scale=2))
+        line["cpu_baseline"] = {"value": ns / (time.perf_counter() - t0), "unit": "rows/s", "cores": 1,
+                                "kind": "port", "sample": f"full build + first {ns} probe rows, oracle hash join "
+                                                          "+ GROUP BY, 1 thread"}
+    return line
+
+
+# ---------------------------------------------------------------------------
+# Workloads: ORDER BY radix sort
+# ---------------------------------------------------------------------------
+def w_sort(c: Ctx, kind: str):
+    a = c.args
+    torch = c.torch
+    dg = datagen()
+    if kind == "i64":
+        n = a.sort_rows
+        keys = np.concatenate([dg.uniform_u64(4, 31, min(1 << 26, n - s), s).view(np.int64)
+                               for s in range(0, n, 1 << 26)])
+        dt, kb, np_ = "i64", 8, 8
+    else:
+        n = a.sortf_rows
+        keys = dg.sort_f32(n, seed=5)
+        dt, kb, np_ = "f32", 4, 4
+    col = c.bolt.Column(torch.from_numpy(keys).to(c.dev), dt)
+    perm = torch.empty(n, dtype=torch.int32, device=c.dev)
+    abi = importlib.import_module("craton_bolt_b200._abi")
+    kv = col.view()
+    pm = abi.ColMut(perm.data_ptr(), None, n, abi.U32, 0)
+    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE
+
+    def step():
+        st = c.lib.bolt_radix_sort_perm(c.eng._ctx, C.byref(kv), 0, 0, C.byref(pm), flags,
+                                        C.c_void_p(c.stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+        return int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
+
+    ms, launches, kms, clocks = c.timed(step, a.steps, a.warmup)
+    # pass accounting: histogram reads keys once; each 8-bit pass reads and
+    # writes (key + u32 payload); the first pass reads only the key, the last
+    # writes only the payload.
+    passes = np_
+    alg = n * (kb + kb + (passes - 2) * 2 * (kb + 4) + (kb + kb + 4) + (kb + 4 + 4))
+    line = base_line(c, ms, n, alg, kms, "sort (histogram + passes)", f"sort_{kind}",
+                     {"workload": f"ORDER BY radix sort: {n} {dt} keys" +
+                                  (" uniform over the full range" if kind == "i64" else
+                                   " incl. negatives, +-0, +-inf, 0.1% NaN"),
+                      "rows": n, "passes": passes, "algorithmic_bytes": alg,
+                      "minimum_bytes": n * (kb + 4), "l2": "inputs larger than L2"},
+                     launches, clocks, dt)
+    if not a.no_cpu:
+        orc = oracle_mod()
+        ns = min(a.cpu_rows, n)
+        t0 = time.perf_counter()
+        orc.sort_perm(orc.HostCol(keys[:ns], dt))
+        line["cpu_baseline"] = {"value": ns / (time.perf_counter() - t0), "unit": "rows/s", "cores": 1,
+                                "kind": "port", "sample": f"first {ns} keys, stable LSD sort in the oracle, 1 thread"}
+    return line
+
+
+# ---------------------------------------------------------------------------
+# Workload: WHERE compaction
+# ---------------------------------------------------------------------------
+def w_compact(c: Ctx):
+    a = c.args
+    torch = c.torch
+    data = gen_filtered(a.rows, c.dev)
+    dev = {k: c.bolt.Column(torch.from_numpy(v).to(c.dev), FILTERED_DT[k]) for k, v in data.items()}
+    abi = importlib.import_module("craton_bolt_b200._abi")
+    names = list(dev)
+    views = (abi.ColView * len(names))(*[dev[k].view() for k in names])
+    outs = {k: torch.empty_like(dev[k].data) for k in names}
+    muts = (abi.ColMut * len(names))(*[abi.ColMut(outs[k].data_ptr(), None, a.rows, abi.DTYPE_CODES[FILTERED_DT[k]], 0)
+                                       for k in names])
+    pred = (abi.Pred * 1)(abi.Pred(names.index("f"), abi.CMP_CODES["<"], 50, 0.0))
+    nout = C.c_uint64(0)
+    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE
+
+    def step():
+        st = c.lib.bolt_compact(c.eng._ctx, views, len(names), pred, 1, muts, None, C.byref(nout), flags,
+                                C.c_void_p(c.stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+        return int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
+
+    ms, launches, kms, clocks = c.timed(step, a.steps, a.warmup)
+    alg = a.rows * FILTERED_BYTES * 1.5  # read all columns, write the ~50% kept
+    return base_line(c, ms, a.rows, alg, kms, "compact_kernel", "compact",
+                     {"workload": "WHERE f < 50 compaction of 5 columns (28 B/row), 100M rows", "rows": a.rows,
+                      "l2": "inputs larger than L2"}, launches, clocks, "mixed")
+
+
+# ---------------------------------------------------------------------------
+# Workload: batched / served stream of filter + GROUP BY queries
+# ---------------------------------------------------------------------------
+CARDS = [10, 32, 100, 316, 1000, 3162, 10_000, 31_623, 100_000, 316_228, 1_000_000]
+
+
+def batch_queries(n_q: int, table_rows: int, seed: int = 7):
+    rng = np.random.default_rng(seed)
+    qs = []
+    for i in range(n_q):
+        rows = int(math.exp(rng.uniform(math.log(1e4), math.log(min(5e7, table_rows)))))
+        begin = int(rng.integers(0, table_rows - rows + 1))
+        card = CARDS[int(rng.integers(0, len(CARDS)))]
+        qs.append({"begin": begin, "end": begin + rows, "card": card, "key": "k32" if i % 2 == 0 else "k64",
+                   "val": "vi" if (i // 2) % 2 == 0 else "vd", "t": int(rng.integers(10, 100))})
+    return qs
+
+
+def w_batch(c: Ctx):
+    a = c.args
+    torch = c.torch
+    dg = datagen()
+    n = a.batch_table_rows
+    base = {"k32": (dg.uniform_u64(8, 1, n) >> np.uint64(33)).astype(np.int64),
+            "vi": (dg.uniform_u64(8, 2, n) % np.uint64(2_000_001)).astype(np.int64) - 1_000_000,
+            "vd": dg.normal_f64(8, 3, n, 1e3),
+            "f": ((dg.uniform_u64(8, 4, n) >> np.uint64(32)) % np.uint64(100)).astype(np.int32)}
+    dev = {"vi": c.bolt.Column(torch.from_numpy(base["vi"]).to(c.dev), "i64"),
+           "vd": c.bolt.Column(torch.from_numpy(base["vd"]).to(c.dev), "f64"),
+           "f": c.bolt.Column(torch.from_numpy(base["f"]).to(c.dev), "i32")}
+    for card in CARDS:
+        kk = base["k32"] % card
+        dev[f"k32_{card}"] = c.bolt.Column(torch.from_numpy(kk.astype(np.int32)).to(c.dev), "i32")
+        dev[f"k64_{card}"] = c.bolt.Column(torch.from_numpy(kk * 1_000_003 - (1 << 40)).to(c.dev), "i64")
+    qs = batch_queries(a.batch_queries, n)
+    total_rows = sum(q["end"] - q["begin"] for q in qs)
+
+    def prep(q):
+        kname = f"{q['key']}_{q['card']}"
+        t = {kname: dev[kname], q["val"]: dev[q["val"]], "f": dev["f"]}
+        return c.eng.prepare_groupby(t, [kname], [("sum", q["val"]), ("count_star", None)], [("f", "<", q["t"])],
+                                     groups_hint=q["card"], rows=(q["begin"], q["end"]))
+
+    prepared = [prep(q) for q in qs]
+    torch.cuda.synchronize()
+    # One at a time: each query through the plain synchronous path.
+    t0 = time.perf_counter()
+    lat_single = []
+    for pq in prepared:
+        s0 = time.perf_counter()
+        st = c.lib.bolt_groupby(c.eng._ctx, C.byref(pq.desc), C.byref(pq.out), 0, C.c_void_p(c.stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+        lat_single.append((time.perf_counter() - s0) * 1e6)
+    single_s = time.perf_counter() - t0
+    single_groups = [int(pq.out.n_groups) for pq in prepared]
+    single_qps = len(qs) / single_s
+    # Served: continuous batching with all queries submitted at once (throughput).
+    scratch = min(a.server_scratch_gb << 30, int(torch.cuda.mem_get_info()[0] * 0.8))
+    srv = c.bolt.Server(c.local, scratch_bytes=scratch, max_batch=a.max_batch, n_lanes=a.lanes)
+    try:
+        prepared2 = [prep(q) for q in qs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tickets = [srv.submit(pq) for pq in prepared2]
+        lat_batch = [srv.wait(t)[1] for t in tickets]
+        batch_s = time.perf_counter() - t0
+        batch_qps = len(qs) / batch_s
+        same = all(int(p2.out.n_groups) == g for p2, g in zip(prepared2, single_groups))
+        # Poisson arrivals at 80% of the one-at-a-time capacity: p50 / p99.
+        rate = 0.8 * single_qps
+        rng = np.random.default_rng(11)
+        gaps = rng.exponential(1.0 / rate, len(qs))
+        prepared3 = [prep(q) for q in qs]
+        torch.cuda.synchronize()
+        tickets = []
+        t0 = time.perf_counter()
+        nxt = t0
+        for pq, gap in zip(prepared3, gaps):
+            nxt += gap
+            while time.perf_counter() < nxt:
+                pass
+            tickets.append(srv.submit(pq))
+        lat_poisson = [srv.wait(t)[1] for t in tickets]
+    finally:
+        srv.close()
+    line = {
+        "metric": METRIC, "value": batch_qps, "unit": "queries/s", "n_gpus": c.world, "steps": 1,
+        "warmup": 0, "ms_per_step": batch_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32/int64/f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{len(qs)} filter + GROUP BY queries over resident {n}-row columns, rows/query "
+                               "log-uniform 1e4..5e7, cardinality log-uniform 10..1e6, int32/int64 keys, "
+                               "int64/f64 values", "rows_total": total_rows, "lanes": a.lanes,
+                   "max_batch": a.max_batch},
+        "batched_qps": batch_qps, "one_at_a_time_qps": single_qps, "speedup": batch_qps / single_qps,
+        "rows_per_s_batched": total_rows / batch_s,
+        "results_equal_alone_vs_mix": same,
+        "latency_us": {"one_at_a_time_p50": float(np.percentile(lat_single, 50)),
+                       "one_at_a_time_p99": float(np.percentile(lat_single, 99)),
+                       "served_poisson_p50": float(np.percentile(lat_poisson, 50)),
+                       "served_poisson_p99": float(np.percentile(lat_poisson, 99)),
+                       "poisson_rate_qps": rate},
+        "gpu_launches": None,
+    }
+    return line
+
+
+WORKLOADS = {"groupby_filtered": w_groupby_filtered, "groupby_plain": w_groupby_plain,
+             "join_groupby": w_join_groupby, "sort_i64": lambda c: w_sort(c, "i64"),
+             "sort_f32": lambda c: w_sort(c, "f32"), "compact": w_compact, "batch": w_batch}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm
+# ---------------------------------------------------------------------------
 def run_reference(args):
     """CPU restatement of the reference's host GROUP BY path, timed per step
     on a bounded sample of the workload's rows."""
     n_sample = args.reference_rows
     data = gen_filtered(n_sample, None)
+    orc = oracle_mod()
+    host = {k: orc.HostCol(np.ascontiguousarray(v), FILTERED_DT[k]) for k, v in data.items()}
     times = []
     for i in range(args.warmup + args.steps):
-        rps, dt = cpu_sample_rows_per_s(data, n_sample)
+        t0 = time.perf_counter()
+        orc.groupby(host, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)])
         if i >= args.warmup:
-            times.append(dt)
+            times.append(time.perf_counter() - t0)
     total = sum(times)
     value = n_sample * len(times) / total
     line = {"metric": METRIC, "value": value, "unit": "rows/s", "impl": "reference", "n_gpus": args.gpus,
@@ -242,8 +697,20 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="groupby_filtered", choices=sorted(WORKLOADS))
     ap.add_argument("--rows", type=int, default=100_000_000)
     ap.add_argument("--groups-hint", type=int, default=4_000_000)
+    ap.add_argument("--plain-rows", type=int, default=1_000_000)
+    ap.add_argument("--build-rows", type=int, default=10_000_000)
+    ap.add_argument("--probe-rows", type=int, default=200_000_000)
+    ap.add_argument("--sort-rows", type=int, default=256 << 20)
+    ap.add_argument("--sortf-rows", type=int, default=64 << 20)
+    ap.add_argument("--batch-queries", type=int, default=4096)
+    ap.add_argument("--batch-table-rows", type=int, default=50_000_000)
+    ap.add_argument("--max-batch", type=int, default=512)
+    ap.add_argument("--lanes", type=int, default=2)
+    ap.add_argument("--server-scratch-gb", type=int, default=64)
+    ap.add_argument("--scratch-gb", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-rows", type=int, default=10_000_000)
     ap.add_argument("--reference-rows", type=int, default=2_000_000)
@@ -252,138 +719,18 @@ def main():
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         if rank == 0:
             run_reference(args)
         return
-
-    import torch
-
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    bolt = load_package()
-    dev = f"cuda:{local}"
-    data = gen_filtered(args.rows, dev)
-    host = {k: torch.from_numpy(v).pin_memory() for k, v in data.items()}
-    dev_cols = {k: bolt.Column(host[k].to(dev), FILTERED_DT[k]) for k in data}
-    torch.cuda.synchronize()
-    eng = bolt.Engine(local, scratch_bytes=8 << 30)
-    call = GroupbyCall(bolt, eng, dev_cols, args.groups_hint, out_cap=max(2 * args.groups_hint, 1 << 20))
-    s = torch.cuda.current_stream(local)
-    flags = bolt.FLAG_ASYNC | bolt.FLAG_PROFILE
-
-    sampler = ClockSampler(local)
-    sampler.start()
-    for _ in range(args.warmup):
-        call(s.cuda_stream, flags)
-    st = eng._lib.bolt_ctx_sync_status(eng._ctx, s.cuda_stream)
-    if st != 0:
-        raise RuntimeError(f"warm-up status {st}: {eng._lib.bolt_ctx_last_error(eng._ctx).decode()}")
-    eng._lib.bolt_ctx_kernel_times(eng._ctx, None, 1 << 20)
-
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches = 0
-    t_wall0 = time.perf_counter()
-    e0.record(s)
-    for _ in range(args.steps):
-        launches += call(s.cuda_stream, flags)
-    e1.record(s)
-    torch.cuda.synchronize()
-    t_wall1 = time.perf_counter()
-    if dist:
-        dist.barrier()
-    ms = e0.elapsed_time(e1)
-    st = eng._lib.bolt_ctx_sync_status(eng._ctx, s.cuda_stream)
-    if st != 0:
-        raise RuntimeError(f"timed-region status {st}: {eng._lib.bolt_ctx_last_error(eng._ctx).decode()}")
-    import ctypes as C
-
-    kt = (C.c_double * 4096)()
-    nk = eng._lib.bolt_ctx_kernel_times(eng._ctx, kt, 4096)
-    kms = [kt[i] for i in range(nk)][-args.steps:]
-    sampler.stop()
-    clocks = sampler.summary(t_wall0, t_wall1)
-    n_groups = int(call.ng.item())
-
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-
-    # End to end through the public API: pinned host columns in, host result out.
-    e2e_ms = None
-    h2d = args.rows * BYTES_PER_ROW
-    d2h = 0
-    if args.e2e_steps > 0:
-        host_cols = {k: bolt.Column(host[k], FILTERED_DT[k]) for k in data}
-        eng.execute_groupby(host_cols, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
-                            groups_hint=args.groups_hint)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(s)
-        for _ in range(args.e2e_steps):
-            r = eng.execute_groupby(host_cols, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
-                                    groups_hint=args.groups_hint)
-        f1.record(s)
-        torch.cuda.synchronize()
-        e2e_ms = f0.elapsed_time(f1) / args.e2e_steps
-        d2h = r.n_groups * (4 + 4 + 8 * 5)
-        if dist:
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-
-    if rank == 0:
-        peak, peak_kind = measured_peak_gbs()
-        alg_bytes = args.rows * BYTES_PER_ROW
-        kern_ms = statistics.mean(kms) if kms else None
-        achieved = alg_bytes / (kern_ms * 1e-3) / 1e9 if kern_ms else None
-        step_ms = ms / args.steps
-        line = {
-            "metric": METRIC, "value": world * args.rows * args.steps / (ms * 1e-3), "unit": "rows/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64",
-            "data": "synthetic (seeded splitmix64 generator; no dataset)",
-            "config": {"workload": "filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) "
-                                   "ranks, WHERE f < 50, SUM/AVG(vd f64), COUNT(*), MIN/MAX(vi i64)",
-                       "rows": args.rows, "groups": n_groups, "groups_hint": args.groups_hint,
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs (2.8 GB) larger than L2 (126 MB); no flush needed"},
-            "hbm_gbs_step": alg_bytes / (step_ms * 1e-3) / 1e9,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None, "traffic": profiled_traffic("groupby_filtered"),
-                         "kernel": "gb_agg_kernel", "kernel_ms": kern_ms,
-                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
-            "gpu_launches": launches,
-            "clocks": clocks,
-            "e2e": {"value": (world * args.rows / (e2e_ms * 1e-3)) if e2e_ms else None, "unit": "rows/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                    "path": "Engine.execute_groupby on pinned host columns (H2D + GROUP BY + D2H)"},
-        }
-        if world == 1 and not args.no_cpu:
-            rps, _ = cpu_sample_rows_per_s(data, min(args.cpu_rows, args.rows))
-            line["cpu_baseline"] = {"value": rps, "unit": "rows/s", "cores": 1, "kind": "port",
-                                    "sample": f"first {min(args.cpu_rows, args.rows)} rows of the workload, CPU "
-                                              "restatement of the reference's host GROUP BY (oracle), 1 thread"}
+    c = Ctx(args)
+    line = WORKLOADS[args.workload](c)
+    if c.rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    c.eng.close()
+    if c.dist:
+        c.dist.barrier()
+        c.dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -28,7 +28,7 @@ from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLO
 
 __all__ = ["BoltError", "DeclineError", "SpillError", "TypeError_", "GpuCapacityError", "TimeoutError_",
            "CudaError", "PlanError", "Column", "Engine", "col", "GroupbyResult", "FLAG_ASYNC",
-           "FLAG_PROFILE", "FLAG_FORCE_GLOBAL", "FLAG_FORCE_SHMEM", "lib"]
+           "FLAG_PROFILE", "FLAG_FORCE_GLOBAL", "FLAG_FORCE_SHMEM", "lib", "PreparedGroupby", "Server"]
 
 
 # ---------------------------------------------------------------------------
@@ -253,6 +253,14 @@ class Engine:
         return Column(t, dtype, v)
 
     # ---- GROUP BY -------------------------------------------------------------
+    def prepare_groupby(self, table: dict, group_by: Sequence[str], aggs: Sequence[tuple],
+                        where: Iterable[tuple] = (), groups_hint: int = 0, out_cap: int | None = None,
+                        rows: tuple[int, int] | None = None) -> "PreparedGroupby":
+        """Builds the C-ABI descriptor and output columns of one GROUP BY
+        (used by execute_groupby, execute_batch and Server.submit)."""
+        cols = {k: self._dev(v) for k, v in table.items()}
+        return PreparedGroupby(self, cols, list(group_by), list(aggs), list(where), int(groups_hint), out_cap, rows)
+
     def try_execute_groupby(self, table: dict, group_by: Sequence[str], aggs: Sequence[tuple],
                             where: Iterable[tuple] = (), groups_hint: int = 0, flags: int = 0,
                             out_cap: int | None = None) -> GroupbyResult | None:
@@ -260,57 +268,18 @@ class Engine:
         (op, column name or None) with op in sum/count/count_star/min/max/avg;
         ``where`` holds (column, cmp, literal) conjuncts. Returns None when the
         shape is declined (the reference's ``Ok(None)``)."""
-        names = list(table.keys())
-        cols = {k: self._dev(v) for k, v in table.items()}
         host_out = not all(v.is_cuda for v in table.values())
-        views = (_abi.ColView * len(names))(*[cols[k].view() for k in names])
-        key_idx = (C.c_int32 * len(group_by))(*[names.index(k) for k in group_by])
-        preds = []
-        for (cname, cmp, lit) in where:
-            c = cols[cname]
-            if c.dtype in ("f32", "f64"):
-                preds.append(_abi.Pred(names.index(cname), CMP_CODES[cmp], 0, float(lit)))
-            else:
-                preds.append(_abi.Pred(names.index(cname), CMP_CODES[cmp], int(lit), 0.0))
-        pred_arr = (_abi.Pred * max(len(preds), 1))(*preds)
-        specs, out_types, nullable = [], [], []
-        for (op, cname) in aggs:
-            op = op.lower()
-            if op == "count" and cname is None:
-                op = "count_star"
-            specs.append(_abi.AggSpec(AGG_CODES[op], names.index(cname) if cname is not None else -1))
-            in_dt = cols[cname].dtype if cname is not None else None
-            out_types.append(_agg_out_dtype(op, in_dt))
-            nullable.append(cname is not None and cols[cname].validity is not None and op not in ("count",))
-        spec_arr = (_abi.AggSpec * len(specs))(*specs)
-        n = len(cols[group_by[0]])
-        desc = _abi.GroupbyDesc(views, len(names), key_idx, len(group_by), pred_arr, len(preds), spec_arr,
-                                len(specs), int(groups_hint))
-        cap = out_cap if out_cap is not None else max(1, min(n + 1, max(2 * groups_hint, 1 << 16)))
+        pq = self.prepare_groupby(table, group_by, aggs, where, groups_hint, out_cap)
         for _attempt in range(2):
-            key_null = len(group_by) == 1 and cols[group_by[0]].validity is not None
-            kout = [self._alloc(cols[k].dtype, cap, key_null) for k in group_by]
-            aout = [self._alloc(t, cap, nb) for t, nb in zip(out_types, nullable)]
-            for c in aout:
-                if c.dtype == "dec128":
-                    c.scale = cols[aggs[aout.index(c)][1]].scale
-            kmut = (_abi.ColMut * len(kout))(*[self._mut(c, cap) for c in kout])
-            amut = (_abi.ColMut * len(aout))(*[self._mut(c, cap) for c in aout])
-            out = _abi.GroupbyOut(kmut, amut, 0, None)
-            st = self._lib.bolt_groupby(self._ctx, C.byref(desc), C.byref(out), flags | FLAG_PROFILE,
+            st = self._lib.bolt_groupby(self._ctx, C.byref(pq.desc), C.byref(pq.out), flags | FLAG_PROFILE,
                                         C.c_void_p(self.stream_handle))
-            if st == _abi.ERR_CAPACITY and out.n_groups > cap:
-                cap = int(out.n_groups)
+            if st == _abi.ERR_CAPACITY and pq.out.n_groups > pq.cap:
+                pq.realloc(int(pq.out.n_groups))
                 continue
             if not self._check(st, "GROUP BY", decline_ok=True):
                 return None
-            g = int(out.n_groups)
-            res = GroupbyResult([self._trim(c, g) for c in kout], [self._trim(c, g) for c in aout], g,
-                                self.last_device_ms, self.last_launches)
-            if host_out:
-                res.keys = [c.to("cpu") for c in res.keys]
-                res.aggs = [c.to("cpu") for c in res.aggs]
-            return res
+            self._lib.bolt_ctx_kernel_times(self._ctx, None, 1 << 20)
+            return pq.result(host_out)
         raise GpuCapacityError("GROUP BY: output capacity retry failed", _abi.ERR_CAPACITY)
 
     def execute_groupby(self, *args, **kw) -> GroupbyResult:
@@ -318,6 +287,19 @@ class Engine:
         if r is None:
             raise DeclineError(f"GROUP BY declined: {self._lib.bolt_ctx_last_error(self._ctx).decode()}")
         return r
+
+    def execute_batch(self, prepared: Sequence["PreparedGroupby"], flags: int = 0) -> list[GroupbyResult]:
+        """Runs many prepared GROUP BY queries as one batch (one persistent
+        aggregation launch + one batched finalize)."""
+        qs = (_abi.Query * len(prepared))(*[pq.query() for pq in prepared])
+        st = self._lib.bolt_batch_groupby(self._ctx, qs, len(prepared), flags, C.c_void_p(self.stream_handle))
+        self._check(st, "batched GROUP BY")
+        out = []
+        for pq, q in zip(prepared, qs):
+            pq.out.n_groups = q.out.n_groups
+            out.append(pq.result(False))
+        return out
+
 
     @staticmethod
     def _mut(c: Column, cap: int) -> _abi.ColMut:
@@ -438,3 +420,110 @@ class Engine:
             return self._trim(g, k), self._trim(s, k), self._trim(c, k)
         finally:
             self._lib.bolt_hash_join_release(self._ctx, table)
+
+
+class PreparedGroupby:
+    """Descriptor + output columns of one GROUP BY through the C ABI. Keeps
+    every buffer the descriptor points to alive."""
+
+    def __init__(self, eng: Engine, cols: dict, group_by, aggs, where, groups_hint, out_cap, rows):
+        self.eng = eng
+        self.cols = cols
+        names = list(cols.keys())
+        self.views = (_abi.ColView * len(names))(*[cols[k].view() for k in names])
+        self.key_idx = (C.c_int32 * len(group_by))(*[names.index(k) for k in group_by])
+        preds = []
+        for (cname, cmp, lit) in where:
+            c = cols[cname]
+            if c.dtype in ("f32", "f64"):
+                preds.append(_abi.Pred(names.index(cname), CMP_CODES[cmp], 0, float(lit)))
+            else:
+                preds.append(_abi.Pred(names.index(cname), CMP_CODES[cmp], int(lit), 0.0))
+        self.preds = (_abi.Pred * max(len(preds), 1))(*preds)
+        specs, self.out_types, self.nullable, self.scales = [], [], [], []
+        for (op, cname) in aggs:
+            op = op.lower()
+            if op == "count" and cname is None:
+                op = "count_star"
+            specs.append(_abi.AggSpec(AGG_CODES[op], names.index(cname) if cname is not None else -1))
+            in_dt = cols[cname].dtype if cname is not None else None
+            self.out_types.append(_agg_out_dtype(op, in_dt))
+            self.nullable.append(cname is not None and cols[cname].validity is not None and op != "count")
+            self.scales.append(cols[cname].scale if cname is not None else 0)
+        self.specs = (_abi.AggSpec * len(specs))(*specs)
+        self.group_by = group_by
+        n = len(cols[group_by[0]])
+        self.rows = rows if rows is not None else (0, n)
+        span = self.rows[1] - self.rows[0]
+        self.desc = _abi.GroupbyDesc(self.views, len(names), self.key_idx, len(group_by), self.preds, len(preds),
+                                     self.specs, len(specs), groups_hint)
+        self.realloc(out_cap if out_cap is not None else max(1, min(span + 1, max(2 * groups_hint, 1 << 16))))
+
+    def realloc(self, cap: int):
+        self.cap = cap
+        e = self.eng
+        key_null = len(self.group_by) == 1 and self.cols[self.group_by[0]].validity is not None
+        self.kout = [e._alloc(self.cols[k].dtype, cap, key_null) for k in self.group_by]
+        self.aout = [e._alloc(t, cap, nb) for t, nb in zip(self.out_types, self.nullable)]
+        for c, sc in zip(self.aout, self.scales):
+            if c.dtype == "dec128":
+                c.scale = sc
+        self.kmut = (_abi.ColMut * len(self.kout))(*[Engine._mut(c, cap) for c in self.kout])
+        self.amut = (_abi.ColMut * len(self.aout))(*[Engine._mut(c, cap) for c in self.aout])
+        self.out = _abi.GroupbyOut(self.kmut, self.amut, 0, None)
+
+    def query(self) -> _abi.Query:
+        return _abi.Query(self.desc, self.out, self.rows[0], self.rows[1], 0)
+
+    def result(self, host_out: bool) -> GroupbyResult:
+        g = int(self.out.n_groups)
+        res = GroupbyResult([Engine._trim(c, g) for c in self.kout], [Engine._trim(c, g) for c in self.aout], g,
+                            self.eng.last_device_ms, self.eng.last_launches)
+        if host_out:
+            res.keys = [c.to("cpu") for c in res.keys]
+            res.aggs = [c.to("cpu") for c in res.aggs]
+        return res
+
+
+class Server:
+    """Continuous-batching request loop (bolt_server_*): queries are admitted
+    by HBM footprint into batches that run on `n_lanes` overlapping streams."""
+
+    def __init__(self, device: int = 0, scratch_bytes: int = 0, max_batch: int = 256, n_lanes: int = 2):
+        self._lib = lib()
+        cfg = _abi.ServerConfig(device, scratch_bytes, max_batch, n_lanes)
+        h = C.c_void_p()
+        st = self._lib.bolt_server_create(C.byref(cfg), C.byref(h))
+        if st != _abi.OK:
+            raise _ERRORS.get(st, BoltError)(f"bolt_server_create failed: {_abi.STATUS_NAMES[st]}", st)
+        self._h = h
+        self._pending = {}
+
+    def submit(self, pq: PreparedGroupby) -> int:
+        q = _abi.Query(pq.desc, pq.out, pq.rows[0], pq.rows[1], 0)
+        t = C.c_uint64(0)
+        st = self._lib.bolt_server_submit(self._h, C.byref(q), C.byref(t))
+        if st != _abi.OK:
+            raise _ERRORS.get(st, BoltError)(f"bolt_server_submit failed: {_abi.STATUS_NAMES[st]}", st)
+        self._pending[int(t.value)] = (pq, q)
+        return int(t.value)
+
+    def wait(self, ticket: int) -> tuple[GroupbyResult, float]:
+        lat = C.c_double(0.0)
+        st = self._lib.bolt_server_wait(self._h, ticket, C.byref(lat))
+        pq, q = self._pending.pop(ticket)
+        if st != _abi.OK:
+            raise _ERRORS.get(st, BoltError)(f"query {ticket} failed: {_abi.STATUS_NAMES[st]}", st)
+        pq.out.n_groups = q.out.n_groups
+        return pq.result(False), float(lat.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bolt_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

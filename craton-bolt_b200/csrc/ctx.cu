@@ -28,6 +28,36 @@ void* arena_alloc(bolt_ctx* ctx, uint64_t bytes) {
     return ctx->arena + off;
 }
 
+bolt_status stage_upload(bolt_ctx* ctx, cudaStream_t s, void* dst, const void* src, uint64_t bytes) {
+    if (bytes == 0) return BOLT_OK;
+    if (bytes > ctx->stage_bytes)
+        return fail(ctx, BOLT_ERR_CAPACITY, "descriptor upload of %llu bytes exceeds the staging ring", (ull)bytes);
+    uint64_t off = (ctx->stage_head + 255) & ~uint64_t(255);
+    if (off + bytes > ctx->stage_bytes) off = 0;
+    // Wait for every earlier upload that overlaps [off, off + bytes).
+    for (uint32_t i = 0; i < bolt_ctx::STAGE_SLOTS; ++i) {
+        auto& u = ctx->stage_use[i];
+        if (u.live && u.off < off + bytes && off < u.off + u.len) {
+            BOLT_CUDA(ctx, cudaEventSynchronize(u.ev));
+            u.live = false;
+        }
+    }
+    auto& slot = ctx->stage_use[ctx->stage_next];
+    if (slot.live) {
+        BOLT_CUDA(ctx, cudaEventSynchronize(slot.ev));
+        slot.live = false;
+    }
+    std::memcpy(ctx->stage + off, src, bytes);
+    BOLT_CUDA(ctx, cudaMemcpyAsync(dst, ctx->stage + off, bytes, cudaMemcpyHostToDevice, s));
+    BOLT_CUDA(ctx, cudaEventRecord(slot.ev, s));
+    slot.off = off;
+    slot.len = bytes;
+    slot.live = true;
+    ctx->stage_next = (ctx->stage_next + 1) % bolt_ctx::STAGE_SLOTS;
+    ctx->stage_head = off + bytes;
+    return BOLT_OK;
+}
+
 bolt_status call_begin(bolt_ctx* ctx, uint32_t flags, cudaStream_t s) {
     arena_reset(ctx);
     ctx->last_error.clear();
@@ -121,13 +151,17 @@ bolt_status bolt_ctx_create(int device, uint64_t scratch_bytes, bolt_ctx** out) 
         [&] {
             for (uint32_t i = 0; i < 2 * bolt_ctx::KRING; ++i)
                 if (cudaEventCreate(&ctx->kev[i]) != cudaSuccess) return true;
+            for (uint32_t i = 0; i < bolt_ctx::STAGE_SLOTS; ++i)
+                if (cudaEventCreateWithFlags(&ctx->stage_use[i].ev, cudaEventDisableTiming) != cudaSuccess) return true;
             return false;
-        }()) {
+        }() ||
+        cudaHostAlloc(&ctx->stage, 32ull << 20, cudaHostAllocDefault) != cudaSuccess) {
         bolt_ctx_destroy(ctx);
         cudaGetLastError();
         return BOLT_ERR_CAPACITY;
     }
     ctx->arena_bytes = scratch_bytes;
+    ctx->stage_bytes = 32ull << 20;
     cudaMemset(ctx->d_status, 0, 16);
     cudaMemset(ctx->d_words, 0, 64 * sizeof(ull));
     cudaDeviceSynchronize();
@@ -146,6 +180,9 @@ void bolt_ctx_destroy(bolt_ctx* ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (uint32_t i = 0; i < 2 * bolt_ctx::KRING; ++i)
         if (ctx->kev[i]) cudaEventDestroy(ctx->kev[i]);
+    for (uint32_t i = 0; i < bolt_ctx::STAGE_SLOTS; ++i)
+        if (ctx->stage_use[i].ev) cudaEventDestroy(ctx->stage_use[i].ev);
+    if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
 }
 

@@ -33,6 +33,17 @@ struct bolt_ctx {
     uint32_t last_launches = 0;
     uint32_t async_pending = 0;
     std::string last_error;
+    // Pinned staging ring for descriptor uploads: each upload copies into the
+    // next free chunk and records an event; a chunk is reused only after its
+    // event completed, so asynchronous calls never see their descriptors
+    // overwritten.
+    static constexpr uint32_t STAGE_SLOTS = 64;
+    char* stage = nullptr;
+    uint64_t stage_bytes = 0;
+    uint64_t stage_head = 0;
+    struct StageUse { uint64_t off, len; cudaEvent_t ev; bool live; };
+    StageUse stage_use[STAGE_SLOTS] = {};
+    uint32_t stage_next = 0;
 };
 
 namespace bolt {
@@ -52,6 +63,10 @@ bolt_status cuda_fail(bolt_ctx* ctx, cudaError_t e, const char* where);
 // Arena allocation (256-byte aligned); returns nullptr when exhausted.
 void* arena_alloc(bolt_ctx* ctx, uint64_t bytes);
 inline void arena_reset(bolt_ctx* ctx) { ctx->arena_used = ctx->arena_pinned; }
+
+// Copies `bytes` of host data to device memory `dst` in stream order through
+// the pinned staging ring (the host buffer may be reused on return).
+bolt_status stage_upload(bolt_ctx* ctx, cudaStream_t s, void* dst, const void* src, uint64_t bytes);
 
 // Begins / ends a call: resets the arena, clears the status word, records the
 // profiling event.

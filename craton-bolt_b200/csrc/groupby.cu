@@ -28,6 +28,7 @@
 // n * 2^-(e+1) of the exact sum. Non-finite or |v| >= 2^32 inputs flag the
 // call and it is re-run with plain f64 atomics (the reference's own method).
 #include "groupby.cuh"
+#include "join.cuh"
 #include "radix_sort.cuh"
 
 #include <algorithm>
@@ -261,25 +262,16 @@ __device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored) {
 // ---------------------------------------------------------------------------
 // Aggregation kernel
 // ---------------------------------------------------------------------------
+// One tile of blockDim.x * U rows starting at row `base` of the query:
+// load, filter, key, pre-aggregate and fold into the shared or global table.
+// `sk` / `sw` are the shared table's keys and state words (C slots, C may be 0).
 template <int U, int MAXS>
-__global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbParams p) {
-    extern __shared__ __align__(16) ull smem[];
-    __shared__ uint32_t s_ins;
-    __shared__ int s_stop;
+__device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull* sw, int C, uint64_t base,
+                                                uint32_t& inserts) {
     const int SW = p.slot_words - 1;
-    const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
-    ull* sk = smem;
-    ull* sw = smem + C;
-    for (int i = threadIdx.x; i < C * (SW + 1); i += blockDim.x) smem[i] = 0;
-    if (threadIdx.x == 0) { s_ins = 0; s_stop = 0; }
-    __syncthreads();
-
     const uint32_t lane = lane_id();
     const uint64_t n = p.n_rows;
-    const uint64_t tile = (uint64_t)blockDim.x * U;
-    uint32_t inserts = 0;
-
-    for (uint64_t base = (uint64_t)blockIdx.x * tile; base < n; base += (uint64_t)gridDim.x * tile) {
+    {
         bool has[U];
         bool knull[U];
         ull stored[U];
@@ -301,7 +293,15 @@ __global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbP
 #pragma unroll
             for (int s = 0; s < MAXS; ++s) raw[u][s] = 0;
             if (!has[u]) continue;
-            stored[u] = ~pack_key(p, r);
+            if (p.jslots) {
+                if (bit_valid(p.jkvalid, r))
+                    stored[u] = p.jkdt == BOLT_I32 ? (ull)(ll)ld_stream((const int32_t*)p.jkey + r)
+                                                   : (ull)ld_stream((const ll*)p.jkey + r);
+                else
+                    has[u] = false;
+            } else {
+                stored[u] = ~pack_key(p, r);
+            }
 #pragma unroll
             for (int s = 0; s < MAXS; ++s) {
                 if (s < p.n_st && p.st[s].col) {
@@ -315,8 +315,20 @@ __global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbP
                 }
             }
             for (int q = 0; q < p.n_pred; ++q) has[u] = has[u] && eval_pred(p.pred[q], r);
-            for (int k = 0; k < p.n_keys; ++k) knull[u] = knull[u] || !bit_valid(p.kvalid[k], r);
+            if (!p.jslots)
+                for (int k = 0; k < p.n_keys; ++k) knull[u] = knull[u] || !bit_valid(p.kvalid[k], r);
             if (knull[u] && p.n_keys > 1) has[u] = false;  // multi-key: NULL-key rows are dropped
+        }
+        if (p.jslots) {
+            // Join source: stored[u] holds the probe key; its group key is the
+            // matched build row's payload. All U lookups are issued together.
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (!has[u]) continue;
+                const ull w1 = join_lookup(p.jslots, p.jlog2cap, stored[u]);
+                if (w1 == ~0ull) has[u] = false;
+                stored[u] = ~(ull)(ll)(int32_t)(uint32_t)w1;
+            }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -384,27 +396,34 @@ __global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbP
                 }
             }
         }
-        // Occupancy accounting: stop early once the table must grow.
-        if (inserts) {
-            atomicAdd(&s_ins, inserts);
-            inserts = 0;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            if (s_ins) {
-                ull tot = atomicAdd(p.occupancy, (ull)s_ins) + s_ins;
-                s_ins = 0;
-                if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
-            }
-            s_stop = (*reinterpret_cast<volatile uint32_t*>(p.status) & (ST_FLAG_GROW | ST_FLAG_SPILL)) != 0;
-        }
-        __syncthreads();
-        if (s_stop) break;
     }
-    if (s_stop) return;
+}
 
-    // Merge the shared-memory table into the global table.
+// Per-tile occupancy accounting (call with the whole CTA): returns true once
+// the query's table must grow or spilled, so the CTA stops early.
+__device__ __forceinline__ bool gb_tile_epilogue(const GbParams& p, uint32_t& inserts, uint32_t* s_ins, int* s_stop) {
+    if (inserts) {
+        atomicAdd(s_ins, inserts);
+        inserts = 0;
+    }
     __syncthreads();
+    if (threadIdx.x == 0) {
+        if (*s_ins) {
+            ull tot = atomicAdd(p.occupancy, (ull)*s_ins) + *s_ins;
+            *s_ins = 0;
+            if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
+        }
+        *s_stop = (*reinterpret_cast<volatile uint32_t*>(p.status) & (ST_FLAG_GROW | ST_FLAG_SPILL)) != 0;
+    }
+    __syncthreads();
+    return *s_stop != 0;
+}
+
+// Merges a CTA's shared table into the query's global table (whole CTA,
+// after a __syncthreads()).
+__device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk, const ull* sw, int C) {
+    const int SW = p.slot_words - 1;
+    uint32_t inserts = 0;
     for (int i = threadIdx.x; i < C; i += blockDim.x) {
         const ull key = sk[i];
         if (key == 0) continue;
@@ -421,6 +440,28 @@ __global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbP
         ull tot = atomicAdd(p.occupancy, (ull)inserts) + inserts;
         if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
     }
+}
+
+template <int U, int MAXS>
+__global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbParams p) {
+    extern __shared__ __align__(16) ull smem[];
+    __shared__ uint32_t s_ins;
+    __shared__ int s_stop;
+    const int SW = p.slot_words - 1;
+    const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
+    ull* sk = smem;
+    ull* sw = smem + C;
+    for (int i = threadIdx.x; i < C * (SW + 1); i += blockDim.x) smem[i] = 0;
+    if (threadIdx.x == 0) { s_ins = 0; s_stop = 0; }
+    __syncthreads();
+    const uint64_t tile = (uint64_t)blockDim.x * U;
+    uint32_t inserts = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * tile; base < p.n_rows; base += (uint64_t)gridDim.x * tile) {
+        gb_process_tile<U, MAXS>(p, sk, sw, C, base, inserts);
+        if (gb_tile_epilogue(p, inserts, &s_ins, &s_stop)) return;
+    }
+    __syncthreads();
+    gb_flush_shared(p, sk, sw, C);
 }
 
 // ---------------------------------------------------------------------------
@@ -514,54 +555,97 @@ __device__ void emit_group(const GbFinal& f, uint64_t o, uint64_t slot) {
     }
 }
 
-// Occupied-slot compaction for the large path; order key = packed ^ sign bit.
-__global__ void __launch_bounds__(256) gb_compact_kernel(GbFinal f) {
-    const ull cap = 1ull << f.log2cap;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base <= cap; base += stride) {
-        const uint64_t i = base + threadIdx.x;
-        bool occ = false;
-        ull ok = 0;
-        if (i < cap) {
-            ull k = ld_volatile(f.gtab + i * (ull)f.slot_words);
-            occ = k != 0;
-            ok = ~k ^ 0x8000000000000000ull;
-        } else if (i == cap) {
-            occ = f.gtab[cap * (ull)f.slot_words] != 0;
-            ok = ~0ull ^ 0x8000000000000000ull;
-        }
-        const uint32_t m = __ballot_sync(0xffffffffu, occ);
-        if (!m) continue;
-        ull pos = 0;
-        if (lane_id() == (uint32_t)(__ffs(m) - 1)) pos = atomicAdd(f.n_nonnull, (ull)__popc(m));
-        pos = __shfl_sync(0xffffffffu, pos, __ffs(m) - 1);
-        if (occ) {
-            pos += __popc(m & lanemask_lt());
-            f.order_keys[pos] = ok;
-            f.slots[pos] = (uint32_t)i;
+// Copies query q's finalize descriptor into shared memory (whole CTA).
+__device__ __forceinline__ void load_final(GbFinal& dst, const GbFinal* src) {
+    const int4* s = reinterpret_cast<const int4*>(src);
+    int4* d = reinterpret_cast<int4*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(GbFinal) / 16); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
+// Index of the query owning flattened work item `item`.
+__device__ __forceinline__ int query_of(const uint32_t* begins, int nq, uint32_t item) {
+    int lo = 0, hi = nq;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(begins + mid) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+constexpr int FIN_CHUNK = 4096;
+
+// Occupied-slot compaction of the large-table queries: work items are
+// (query, chunk of 4096 slots); order key = packed key ^ sign bit.
+__global__ void __launch_bounds__(256) gb_compact_batch_kernel(const GbFinal* fins, const uint32_t* begins, int nq,
+                                                                uint32_t total_items) {
+    __shared__ __align__(16) GbFinal f;
+    for (uint32_t item = blockIdx.x; item < total_items; item += gridDim.x) {
+        const int q = query_of(begins, nq, item);
+        __syncthreads();
+        load_final(f, fins + q);
+        const ull cap = 1ull << f.log2cap;
+        const uint64_t c0 = (uint64_t)(item - begins[q]) * FIN_CHUNK;
+        const uint64_t c1 = c0 + FIN_CHUNK < cap + 1 ? c0 + FIN_CHUNK : cap + 1;
+        for (uint64_t base = c0; base < c1; base += blockDim.x) {
+            const uint64_t i = base + threadIdx.x;
+            bool occ = false;
+            ull ok = 0;
+            if (i < cap) {
+                const ull k = ld_volatile(f.gtab + i * (ull)f.slot_words);
+                occ = k != 0;
+                ok = ~k ^ 0x8000000000000000ull;
+            } else if (i == cap) {
+                occ = f.gtab[cap * (ull)f.slot_words] != 0;
+                ok = ~0ull ^ 0x8000000000000000ull;
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, occ);
+            if (!m) continue;
+            ull pos = 0;
+            if (lane_id() == (uint32_t)(__ffs(m) - 1)) pos = atomicAdd(f.n_nonnull, (ull)__popc(m));
+            pos = __shfl_sync(0xffffffffu, pos, __ffs(m) - 1);
+            if (occ) {
+                pos += __popc(m & lanemask_lt());
+                f.order_keys[pos] = ok;
+                f.slots[pos] = (uint32_t)i;
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(256) gb_gather_kernel(GbFinal f) {
-    const ull cap = 1ull << f.log2cap;
-    const ull G = *f.n_nonnull;
-    const bool has_null = f.gtab[(cap + 1) * (ull)f.slot_words] != 0;
-    const ull total = G + (has_null ? 1 : 0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *f.n_groups = total;
-        if (f.n_groups_user) *f.n_groups_user = total;
-        if (total > f.out_cap) atomicOr(f.status, ST_FLAG_CAPACITY);
+// Output rows of the large-table queries: work items are (query, chunk of
+// 4096 output rows) up to cap + 1 rows; rows past the group count exit.
+__global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fins, const uint32_t* begins, int nq,
+                                                               uint32_t total_items) {
+    __shared__ __align__(16) GbFinal f;
+    for (uint32_t item = blockIdx.x; item < total_items; item += gridDim.x) {
+        const int q = query_of(begins, nq, item);
+        __syncthreads();
+        load_final(f, fins + q);
+        const ull cap = 1ull << f.log2cap;
+        const ull G = *f.n_nonnull;
+        const bool has_null = f.gtab[(cap + 1) * (ull)f.slot_words] != 0;
+        const ull total = G + (has_null ? 1 : 0);
+        const uint64_t c0 = (uint64_t)(item - begins[q]) * FIN_CHUNK;
+        if (c0 == 0 && threadIdx.x == 0) {
+            *f.n_groups = total;
+            if (f.n_groups_user) *f.n_groups_user = total;
+            if (total > f.out_cap) atomicOr(f.status, ST_FLAG_CAPACITY);
+        }
+        const ull lim = total < f.out_cap ? total : f.out_cap;
+        const uint64_t c1 = c0 + FIN_CHUNK < lim ? c0 + FIN_CHUNK : lim;
+        for (uint64_t o = c0 + threadIdx.x; o < c1; o += blockDim.x) emit_group(f, o, o < G ? f.sorted[o] : cap + 1);
     }
-    const ull lim = total < f.out_cap ? total : f.out_cap;
-    for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < lim; o += (uint64_t)gridDim.x * blockDim.x)
-        emit_group(f, o, o < G ? f.sorted[o] : cap + 1);
 }
 
-// One CTA: compact + bitonic sort in shared memory + emit (tables <= 8192 slots).
-__global__ void __launch_bounds__(1024) gb_small_final_kernel(GbFinal f) {
+// One CTA per small-table query (<= 8192 slots): compact + bitonic sort in
+// shared memory + emit.
+__global__ void __launch_bounds__(1024) gb_small_final_kernel(const GbFinal* fins) {
     extern __shared__ __align__(16) ull sm[];
     __shared__ uint32_t s_n;
+    __shared__ __align__(16) GbFinal f;
+    load_final(f, fins + blockIdx.x);
     const ull cap = 1ull << f.log2cap;
     const uint32_t P = (uint32_t)cap * 2;  // power of two >= cap + 1
     ull* key = sm;
@@ -624,12 +708,55 @@ bolt_status launch_agg(bolt_ctx* ctx, const GbPlan& pl, cudaStream_t s, size_t s
     return BOLT_OK;
 }
 
-int dtype_size(int dt) {
-    switch (dt) {
-    case BOLT_I32: case BOLT_F32: case BOLT_U32: return 4;
-    case BOLT_DEC128: return 16;
-    default: return 8;
+// Persistent multi-query aggregation: work items are (query, tile of
+// blockDim.x * U rows) handed out in order from one counter. A CTA keeps one
+// query's shared table while its items stay on that query and merges it into
+// that query's global table when it moves on. Each query has its own table,
+// occupancy and status words, so one query's spill never touches another's.
+template <int U, int MAXS>
+__global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms, const uint32_t* begins, int nq,
+                                                           uint32_t total_items, uint32_t* counter) {
+    extern __shared__ __align__(16) ull smem[];
+    __shared__ __align__(16) GbParams p;
+    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_ins;
+    __shared__ int s_stop;
+    int cur = -1;
+    int C = 0;
+    uint32_t inserts = 0;
+    if (threadIdx.x == 0) {
+        s_ins = 0;
+        s_stop = 0;
     }
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= total_items) break;
+        const int q = query_of(begins, nq, item);
+        if (q != cur) {
+            if (cur >= 0) {
+                gb_flush_shared(p, smem, smem + C, C);
+                __syncthreads();
+            }
+            const int4* src = reinterpret_cast<const int4*>(prms + q);
+            int4* dst = reinterpret_cast<int4*>(&p);
+            for (int i = threadIdx.x; i < (int)(sizeof(GbParams) / 16); i += blockDim.x) dst[i] = src[i];
+            if (threadIdx.x == 0) s_stop = 0;
+            __syncthreads();
+            C = p.smem_log2 ? (1 << p.smem_log2) : 0;
+            for (int i = threadIdx.x; i < C * p.slot_words; i += blockDim.x) smem[i] = 0;
+            __syncthreads();
+            cur = q;
+        } else if (s_stop) {
+            __syncthreads();
+            continue;  // the query already flagged growth; the host re-runs it
+        }
+        const uint64_t base = (uint64_t)(item - begins[q]) * blockDim.x * U;
+        gb_process_tile<U, MAXS>(p, smem, smem + C, C, base, inserts);
+        gb_tile_epilogue(p, inserts, &s_ins, &s_stop);
+    }
+    if (cur >= 0) gb_flush_shared(p, smem, smem + C, C);
 }
 
 }  // namespace
@@ -816,34 +943,70 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
 }
 
 uint64_t gb_plan_scratch(const GbPlan& pl) {
-    const uint64_t table = (pl.cap + 2) * (uint64_t)pl.prm.slot_words * 8 + 256;
-    if (pl.small_final) return table + 1024;
+    const uint64_t table = (pl.cap + 2) * (uint64_t)pl.prm.slot_words * 8 + 256 + 64;
+    if (pl.small_final) return table + sizeof(GbFinal) + 512;
     const uint64_t g = pl.cap + 1;
-    return table + g * 8 + g * 4 + g * 4 + radix_sort_scratch(g, SRC_U64_KEYS) + 4096;
+    return table + g * 16 + 1024 + sizeof(GbFinal) + radix_sort_scratch(g, 1, SRC_U64_KEYS);
 }
 
-bolt_status gb_enqueue(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s) {
-    GbParams& p = pl->prm;
-    GbFinal& f = pl->fin;
-    const uint64_t table_bytes = (pl->cap + 2) * (uint64_t)p.slot_words * 8;
-    p.gtab = (ull*)arena_alloc(ctx, table_bytes);
-    ull* words = (ull*)arena_alloc(ctx, 256);
-    if (!p.gtab || !words)
-        return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for a %llu-slot table",
-                    (ull)pl->cap);
-    p.occupancy = words;
-    f.gtab = p.gtab;
-    f.n_nonnull = words + 1;
-    f.n_groups = words + 2;
-    BOLT_CUDA(ctx, cudaMemsetAsync(p.gtab, 0, table_bytes, s));
-    BOLT_CUDA(ctx, cudaMemsetAsync(words, 0, 256, s));
+namespace {
 
-    const size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
-    // Grid: resident CTAs on every SM, no more than the tiles.
-    const uint64_t tile = (uint64_t)pl->block * pl->u;
-    const uint64_t tiles = (p.n_rows + tile - 1) / tile;
+template <int U, int MAXS>
+bolt_status launch_batch_agg(bolt_ctx* ctx, cudaStream_t s, const GbParams* d_prms, const uint32_t* d_begins, int nq,
+                             uint32_t items, uint32_t* counter, size_t smem, int block) {
+    auto kfn = gb_batch_agg_kernel<U, MAXS>;
+    BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
-    {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, items);
+    kfn<<<grid, block, smem, s>>>(d_prms, d_begins, nq, items, counter);
+    ctx->last_launches++;
+    return BOLT_OK;
+}
+
+}  // namespace
+
+bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
+    if (nq <= 0) return BOLT_OK;
+    // Tables and per-query words (occupancy, groups, status) in one zeroed region.
+    std::vector<uint64_t> toff(nq);
+    uint64_t tot = 0;
+    for (int q = 0; q < nq; ++q) {
+        toff[q] = tot;
+        tot += ((pls[q]->cap + 2) * (uint64_t)pls[q]->prm.slot_words * 8 + 255) & ~uint64_t(255);
+    }
+    const uint64_t words_off = tot;
+    tot += (uint64_t)nq * 64;
+    char* region = (char*)arena_alloc(ctx, tot);
+    if (!region)
+        return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for %d table(s) of %llu bytes", nq,
+                    (ull)tot);
+    BOLT_CUDA(ctx, cudaMemsetAsync(region, 0, tot, s));
+    for (int q = 0; q < nq; ++q) {
+        GbParams& p = pls[q]->prm;
+        GbFinal& f = pls[q]->fin;
+        ull* w = (ull*)(region + words_off) + 8 * q;
+        p.gtab = (ull*)(region + toff[q]);
+        p.occupancy = w;
+        // A single query reports through the context's status word (so
+        // bolt_ctx_sync_status sees it); batched queries each get their own.
+        p.status = nq == 1 ? ctx->d_status : (uint32_t*)(w + 3);
+        f.gtab = p.gtab;
+        f.n_nonnull = w + 1;
+        f.n_groups = w + 2;
+        f.status = p.status;
+        pls[q]->words = w;
+    }
+
+    // Aggregation.
+    if (nq == 1) {
+        GbPlan* pl = pls[0];
+        GbParams& p = pl->prm;
+        const size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
+        const uint64_t tile = (uint64_t)pl->block * pl->u;
+        const uint64_t tiles = (p.n_rows + tile - 1) / tile;
+        int per_sm = 1;
         cudaError_t e;
         if (pl->u == 4) {
             BOLT_CUDA(ctx, cudaFuncSetAttribute(gb_agg_kernel<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -853,41 +1016,112 @@ bolt_status gb_enqueue(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb_agg_kernel<2, 8>, pl->block, smem);
         }
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-    }
-    uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
-    if (pl->grid > 0) grid = std::min<uint64_t>(grid, (uint64_t)pl->grid);
-    pl->grid = (int)grid;
-    if (p.n_rows > 0) {
-        kernel_mark_begin(ctx, pl->flags, s);
-        bolt_status st = pl->u == 4 ? launch_agg<4, 4>(ctx, *pl, s, smem) : launch_agg<2, 8>(ctx, *pl, s, smem);
-        kernel_mark_end(ctx, pl->flags, s);
+        uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
+        if (pl->grid > 0) grid = std::min<uint64_t>(grid, (uint64_t)pl->grid);
+        pl->grid = (int)grid;
+        if (p.n_rows > 0) {
+            kernel_mark_begin(ctx, flags, s);
+            bolt_status st = pl->u == 4 ? launch_agg<4, 4>(ctx, *pl, s, smem) : launch_agg<2, 8>(ctx, *pl, s, smem);
+            kernel_mark_end(ctx, flags, s);
+            if (st != BOLT_OK) return st;
+        }
+    } else {
+        int u = 4;
+        size_t smem = 0;
+        for (int q = 0; q < nq; ++q) {
+            if (pls[q]->prm.n_st > 4) u = 2;
+            smem = std::max<size_t>(smem, (size_t)pls[q]->smem_entries * 8 * (size_t)pls[q]->prm.slot_words);
+        }
+        std::vector<GbParams> prms(nq);
+        std::vector<uint32_t> begins(nq + 1);
+        uint64_t items = 0;
+        const uint64_t tile = 512ull * u;
+        for (int q = 0; q < nq; ++q) {
+            prms[q] = pls[q]->prm;
+            begins[q] = (uint32_t)items;
+            items += (pls[q]->prm.n_rows + tile - 1) / tile;
+        }
+        begins[nq] = (uint32_t)items;
+        if (items >= (1ull << 32)) return fail(ctx, BOLT_DECLINE, "batched GROUP BY: too many row tiles");
+        GbParams* d_prms = (GbParams*)arena_alloc(ctx, sizeof(GbParams) * nq);
+        uint32_t* d_begins = (uint32_t*)arena_alloc(ctx, 4ull * (nq + 1) + 64);
+        if (!d_prms || !d_begins) return fail(ctx, BOLT_ERR_CAPACITY, "batched GROUP BY: scratch arena too small");
+        uint32_t* counter = d_begins + nq + 1;
+        bolt_status st = stage_upload(ctx, s, d_prms, prms.data(), sizeof(GbParams) * nq);
+        if (st == BOLT_OK) st = stage_upload(ctx, s, d_begins, begins.data(), 4ull * (nq + 1));
         if (st != BOLT_OK) return st;
+        BOLT_CUDA(ctx, cudaMemsetAsync(counter, 0, 4, s));
+        if (items) {
+            kernel_mark_begin(ctx, flags, s);
+            st = u == 4 ? launch_batch_agg<4, 4>(ctx, s, d_prms, d_begins, nq, (uint32_t)items, counter, smem, 512)
+                        : launch_batch_agg<2, 8>(ctx, s, d_prms, d_begins, nq, (uint32_t)items, counter, smem, 512);
+            kernel_mark_end(ctx, flags, s);
+            if (st != BOLT_OK) return st;
+        }
     }
 
-    if (pl->small_final) {
-        const size_t fsm = (size_t)pl->cap * 2 * 12;
+    // Finalize: small tables one CTA each; large tables through batched
+    // compaction, a segmented radix sort and a batched gather.
+    std::vector<GbFinal> small, large;
+    std::vector<int> large_q;
+    uint64_t small_cap = 0;
+    for (int q = 0; q < nq; ++q) {
+        if (pls[q]->small_final) {
+            small.push_back(pls[q]->fin);
+            small_cap = std::max<uint64_t>(small_cap, pls[q]->cap);
+        } else {
+            large_q.push_back(q);
+        }
+    }
+    if (!small.empty()) {
+        GbFinal* d_f = (GbFinal*)arena_alloc(ctx, sizeof(GbFinal) * small.size());
+        if (!d_f) return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
+        bolt_status st = stage_upload(ctx, s, d_f, small.data(), sizeof(GbFinal) * small.size());
+        if (st != BOLT_OK) return st;
+        const size_t fsm = (size_t)small_cap * 2 * 12;
         BOLT_CUDA(ctx, cudaFuncSetAttribute(gb_small_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-        gb_small_final_kernel<<<1, 1024, fsm, s>>>(f);
+        gb_small_final_kernel<<<(unsigned)small.size(), 1024, fsm, s>>>(d_f);
         ctx->last_launches++;
-    } else {
-        const uint64_t g = pl->cap + 1;
-        f.order_keys = (ull*)arena_alloc(ctx, g * 8);
-        f.slots = (uint32_t*)arena_alloc(ctx, g * 4);
-        f.sorted = (uint32_t*)arena_alloc(ctx, g * 4);
-        if (!f.order_keys || !f.slots || !f.sorted)
-            return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
-        gb_compact_kernel<<<grid_for(g, 256, ctx->num_sms * 8), 256, 0, s>>>(f);
-        ctx->last_launches++;
+    }
+    if (!large_q.empty()) {
+        const int nl = (int)large_q.size();
+        std::vector<uint32_t> cbeg(nl + 1), gbeg(nl + 1);
+        uint64_t citems = 0;
         SortSpec sp;
         sp.src = SRC_U64_KEYS;
-        sp.keys = f.order_keys;
-        sp.payload_in = f.slots;
-        sp.n = g;
-        sp.n_dev = f.n_nonnull;
-        sp.payload_out = f.sorted;
-        bolt_status st = radix_sort(ctx, s, sp);
+        for (int i = 0; i < nl; ++i) {
+            GbPlan* pl = pls[large_q[i]];
+            GbFinal& f = pl->fin;
+            const uint64_t g = pl->cap + 1;
+            f.order_keys = (ull*)arena_alloc(ctx, g * 8);
+            f.slots = (uint32_t*)arena_alloc(ctx, g * 4);
+            f.sorted = (uint32_t*)arena_alloc(ctx, g * 4);
+            if (!f.order_keys || !f.slots || !f.sorted)
+                return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
+            large.push_back(f);
+            cbeg[i] = (uint32_t)citems;
+            citems += (g + FIN_CHUNK - 1) / FIN_CHUNK;
+            SortSegment seg;
+            seg.keys = f.order_keys;
+            seg.payload_in = f.slots;
+            seg.payload_out = f.sorted;
+            seg.n_dev = f.n_nonnull;
+            seg.n = g;
+            sp.segs.push_back(seg);
+        }
+        cbeg[nl] = (uint32_t)citems;
+        GbFinal* d_f = (GbFinal*)arena_alloc(ctx, sizeof(GbFinal) * nl);
+        uint32_t* d_beg = (uint32_t*)arena_alloc(ctx, 4ull * (nl + 1));
+        if (!d_f || !d_beg) return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
+        bolt_status st = stage_upload(ctx, s, d_f, large.data(), sizeof(GbFinal) * nl);
+        if (st == BOLT_OK) st = stage_upload(ctx, s, d_beg, cbeg.data(), 4ull * (nl + 1));
         if (st != BOLT_OK) return st;
-        gb_gather_kernel<<<grid_for(g, 256, ctx->num_sms * 8), 256, 0, s>>>(f);
+        const unsigned cg = (unsigned)std::min<uint64_t>(citems, (uint64_t)ctx->num_sms * 8);
+        gb_compact_batch_kernel<<<cg, 256, 0, s>>>(d_f, d_beg, nl, (uint32_t)citems);
+        ctx->last_launches++;
+        st = radix_sort(ctx, s, sp);
+        if (st != BOLT_OK) return st;
+        gb_gather_batch_kernel<<<cg, 256, 0, s>>>(d_f, d_beg, nl, (uint32_t)citems);
         ctx->last_launches++;
     }
     BOLT_CUDA(ctx, cudaGetLastError());
@@ -905,27 +1139,36 @@ extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64
     const uint64_t groups = desc->groups_hint ? desc->groups_hint : std::min<uint64_t>(n_rows, 1ull << 15);
     const uint64_t cap = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * groups + 16, 64));
     uint64_t bytes = (cap + 2) * words * 8 + 4096;
-    if (cap > 8192) bytes += (cap + 1) * 16 + radix_sort_scratch(cap + 1, SRC_U64_KEYS);
+    if (cap > 8192) bytes += (cap + 1) * 16 + radix_sort_scratch(cap + 1, 1, SRC_U64_KEYS);
     return bytes;
 }
 
-extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc, bolt_groupby_out* out,
-                                    uint32_t flags, bolt_stream stream) {
-    if (!ctx || !desc || !out) return BOLT_ERR_INVALID;
-    cudaStream_t s = (cudaStream_t)stream;
-    uint64_t nrows = 0;
-    if (desc->n_keys >= 1 && desc->key_cols && desc->cols && desc->key_cols[0] >= 0 && desc->key_cols[0] < desc->n_cols)
-        nrows = desc->cols[desc->key_cols[0]].len;
+namespace bolt {
+
+// Runs one query (optionally with a join table as its key source) with the
+// retry policy: grow the table on GROW / SPILL, switch the f64 SUM to atomics
+// on RANGE, switch Decimal128 SUM to the wide state on DECRANGE.
+static bolt_status gb_single(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_groupby_out* out, uint64_t rb,
+                             uint64_t re, uint32_t flags, cudaStream_t s, const bolt_join_table* jt,
+                             const bolt_col_view* jkey, const char* op) {
     int mode = 0;
     uint64_t cap_override = 0;
     for (int attempt = 0; attempt < 6; ++attempt) {
         bolt_status st = call_begin(ctx, flags, s);
         if (st != BOLT_OK) return st;
         GbPlan pl;
-        st = gb_plan(ctx, desc, out, 0, nrows, flags, mode, cap_override, &pl);
+        st = gb_plan(ctx, d, out, rb, re, flags, mode, cap_override, &pl);
         if (st != BOLT_OK) return st;
+        if (jt) {
+            pl.prm.jslots = jt->slots;
+            pl.prm.jlog2cap = jt->log2cap;
+            pl.prm.jkdt = jkey->dtype;
+            pl.prm.jkey = jkey->data;
+            pl.prm.jkvalid = jkey->validity;
+        }
         pl.fin.n_groups_user = (flags & BOLT_FLAG_ASYNC) ? (ull*)out->n_groups_dev : nullptr;
-        st = gb_enqueue(ctx, &pl, s);
+        GbPlan* one = &pl;
+        st = gb_run(ctx, &one, 1, s, flags);
         if (st != BOLT_OK) return st;
         st = call_end(ctx, flags, s);
         if (st != BOLT_OK) return st;
@@ -933,11 +1176,12 @@ extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc
         uint32_t f = 0;
         st = read_status(ctx, s, 0, &f);
         if (st != BOLT_OK) return st;
-        ull ng = 0;
-        BOLT_CUDA(ctx, cudaMemcpy(&ng, pl.fin.n_groups, 8, cudaMemcpyDeviceToHost));
-        out->n_groups = ng;
+        ull w[4] = {0, 0, 0, 0};
+        BOLT_CUDA(ctx, cudaMemcpy(w, pl.words, sizeof w, cudaMemcpyDeviceToHost));
+        out->n_groups = w[2];
         if (f & (ST_FLAG_GROW | ST_FLAG_SPILL)) {
-            if (flags & BOLT_FLAG_FORCE_SHMEM) return fail(ctx, BOLT_ERR_SPILL, "partition_reduce spill: shared-memory tier overflow");
+            if (flags & BOLT_FLAG_FORCE_SHMEM)
+                return fail(ctx, BOLT_ERR_SPILL, "partition_reduce spill: shared-memory tier overflow");
             cap_override = pl.cap * 8;
             continue;
         }
@@ -948,7 +1192,115 @@ extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc
         }
         if (f & ST_FLAG_DECOVERFLOW)
             return fail(ctx, BOLT_ERR_OVERFLOW, "SUM(Decimal128) precision overflow: accumulator exceeds i128 range");
-        return flags_to_status(ctx, f, "GROUP BY");
+        return flags_to_status(ctx, f, op);
     }
-    return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: table growth did not converge");
+    return fail(ctx, BOLT_ERR_CAPACITY, "%s: table growth did not converge", op);
 }
+
+}  // namespace bolt
+
+extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc, bolt_groupby_out* out,
+                                    uint32_t flags, bolt_stream stream) {
+    if (!ctx || !desc || !out) return BOLT_ERR_INVALID;
+    uint64_t nrows = 0;
+    if (desc->n_keys >= 1 && desc->key_cols && desc->cols && desc->key_cols[0] >= 0 && desc->key_cols[0] < desc->n_cols)
+        nrows = desc->cols[desc->key_cols[0]].len;
+    return gb_single(ctx, desc, out, 0, nrows, flags, (cudaStream_t)stream, nullptr, nullptr, "GROUP BY");
+}
+
+// Fused probe -> GROUP BY <build payload>: the GROUP BY kernel with a join
+// lookup as its key source; the joined rows are never materialised.
+extern "C" bolt_status bolt_join_groupby(bolt_ctx* ctx, const bolt_join_table* t, const bolt_col_view* probe_key,
+                                         const bolt_col_view* value, bolt_col_mut* out_group, bolt_col_mut* out_sum,
+                                         bolt_col_mut* out_count, uint64_t* n_groups, uint32_t flags,
+                                         bolt_stream stream) {
+    if (!ctx) return BOLT_ERR_INVALID;
+    if (!t || !probe_key || !value || !out_group || !out_sum || !out_count || !n_groups)
+        return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: bad arguments");
+    if (!t->has_payload) return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: the table was built without a payload");
+    if (probe_key->dtype != BOLT_I32 && probe_key->dtype != BOLT_I64)
+        return fail(ctx, BOLT_DECLINE, "join GROUP BY: probe key dtype %d", probe_key->dtype);
+    if (value->len != probe_key->len) return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: column lengths differ");
+    // Column 0 stands for the group key (its data is never read in join mode).
+    bolt_col_view cols[2] = {*probe_key, *value};
+    cols[0].dtype = BOLT_I32;
+    cols[0].validity = nullptr;
+    const int32_t key_cols[1] = {0};
+    const bolt_agg_spec aggs[2] = {{BOLT_AGG_SUM, 1}, {BOLT_AGG_COUNT_STAR, -1}};
+    bolt_groupby_desc d{};
+    d.cols = cols;
+    d.n_cols = 2;
+    d.key_cols = key_cols;
+    d.n_keys = 1;
+    d.aggs = aggs;
+    d.n_aggs = 2;
+    d.groups_hint = std::min<uint64_t>(std::max<uint64_t>(t->n_build, 1), 2048);
+    bolt_col_mut agg_out[2] = {*out_sum, *out_count};
+    bolt_groupby_out o{};
+    o.keys = out_group;
+    o.aggs = agg_out;
+    bolt_status st = gb_single(ctx, &d, &o, 0, probe_key->len, flags, (cudaStream_t)stream, t, probe_key,
+                               "join GROUP BY");
+    *n_groups = o.n_groups;
+    return st;
+}
+
+// Many filter + GROUP BY queries: one persistent aggregation launch and one
+// batched finalize for the whole batch; queries that need a bigger table or
+// another accumulator mode are re-run alone afterwards.
+extern "C" bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* qs, int32_t n, uint32_t flags,
+                                          bolt_stream stream) {
+    if (!ctx) return BOLT_ERR_INVALID;
+    if (!qs || n < 0) return fail(ctx, BOLT_ERR_INVALID, "batched GROUP BY: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    bolt_status st = call_begin(ctx, flags, s);
+    if (st != BOLT_OK) return st;
+    std::vector<GbPlan> plans(n);
+    std::vector<GbPlan*> run;
+    std::vector<int> idx;
+    for (int i = 0; i < n; ++i) {
+        bolt_query& q = qs[i];
+        q.status = gb_plan(ctx, &q.desc, &q.out, q.row_begin, q.row_end, flags, 0, 0, &plans[i]);
+        if (q.status != BOLT_OK) continue;
+        plans[i].fin.n_groups_user = (ull*)q.out.n_groups_dev;
+        run.push_back(&plans[i]);
+        idx.push_back(i);
+    }
+    st = gb_run(ctx, run.data(), (int)run.size(), s, flags);
+    if (st != BOLT_OK) return st;
+    st = call_end(ctx, flags, s);
+    if (st != BOLT_OK) return st;
+    if (flags & BOLT_FLAG_ASYNC) return BOLT_OK;
+    uint32_t gf = 0;
+    st = read_status(ctx, s, 0, &gf);
+    if (st != BOLT_OK) return st;
+    if (gf & ST_FLAG_TIMEOUT) return flags_to_status(ctx, gf, "batched GROUP BY");
+    const int m = (int)run.size();
+    std::vector<ull> w((size_t)m * 8);
+    if (m) BOLT_CUDA(ctx, cudaMemcpy(w.data(), run[0]->words, (size_t)m * 64, cudaMemcpyDeviceToHost));
+    std::vector<int> redo;
+    for (int j = 0; j < m; ++j) {
+        bolt_query& q = qs[idx[j]];
+        const uint32_t f = (uint32_t)w[(size_t)j * 8 + 3];
+        q.out.n_groups = w[(size_t)j * 8 + 2];
+        if (f & (ST_FLAG_GROW | ST_FLAG_SPILL | ST_FLAG_RANGE | ST_FLAG_DECRANGE)) {
+            redo.push_back(idx[j]);
+            continue;
+        }
+        if (f & ST_FLAG_DECOVERFLOW) q.status = BOLT_ERR_OVERFLOW;
+        else if (f & ST_FLAG_OVERFLOW) q.status = BOLT_ERR_OVERFLOW;
+        else if (f & ST_FLAG_CAPACITY) q.status = BOLT_ERR_CAPACITY;
+        else q.status = BOLT_OK;
+    }
+    for (int i : redo) {
+        bolt_query& q = qs[i];
+        q.status = gb_single(ctx, &q.desc, &q.out, q.row_begin, q.row_end, flags & ~BOLT_FLAG_PROFILE, s, nullptr,
+                             nullptr, "batched GROUP BY");
+    }
+    ctx->last_error.clear();
+    for (int i = 0; i < n; ++i)
+        if (qs[i].status != BOLT_OK)
+            return fail(ctx, qs[i].status, "batched GROUP BY: query %d failed (%s)", i, bolt_status_str(qs[i].status));
+    return BOLT_OK;
+}
+

@@ -77,6 +77,14 @@ struct GbParams {
     uint32_t* status;
     ull* occupancy;
     ull grow_limit;
+    // Join source: when jslots is set the group key of a row is the payload
+    // of the build slot its probe key matches (rows without a match are
+    // skipped) instead of its packed key columns.
+    const ull* jslots;
+    int32_t jlog2cap;
+    int32_t jkdt;
+    const void* jkey;
+    const uint8_t* jkvalid;
 };
 
 struct GbFinal {
@@ -114,6 +122,7 @@ struct GbPlan {
     bool small_final = false;
     int32_t mode = 0;
     uint32_t flags = 0;
+    ull* words = nullptr;  // device: [0] occupancy, [1] non-NULL groups, [2] groups, [3] status
 };
 
 // Plan modes selected after a flagged first attempt.
@@ -128,7 +137,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* desc, const bolt_gro
 // Bytes of scratch the plan needs (table + finalize buffers).
 uint64_t gb_plan_scratch(const GbPlan& plan);
 
-// Allocates scratch and enqueues table init, aggregation and finalize.
-bolt_status gb_enqueue(bolt_ctx* ctx, GbPlan* plan, cudaStream_t s);
+// Allocates scratch and enqueues table init, aggregation and finalize of
+// `nq` planned queries (one persistent aggregation launch when nq > 1).
+bolt_status gb_run(bolt_ctx* ctx, GbPlan** plans, int nq, cudaStream_t s, uint32_t flags);
 
 }  // namespace bolt

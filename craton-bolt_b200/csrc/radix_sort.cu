@@ -1,19 +1,27 @@
-// radix_sort.cu — onesweep LSD radix sort producing a stable permutation.
+// radix_sort.cu — onesweep LSD radix sort producing stable permutations for
+// one or many independent segments at once.
 //
 // Replaces the reference's 4-bit LSD radix with a host scan per pass
 // (src/exec/gpu_sort.rs:995-1230, src/jit/sort_kernel_radix.rs:489-991):
 //   * one histogram kernel reads the keys once and counts all digit
-//     positions (8-bit digits: 4 passes for 32-bit keys, 8 for 64-bit);
-//   * one kernel per digit: tiles of 4096 keys are taken in arrival order,
-//     ranked per warp with __match_any_sync (stable: element order within a
-//     warp's segment, warps in segment order), their digit counts chained
-//     across tiles with decoupled look-back (Merrill & Garland 2016), staged
+//     positions of every segment (8-bit digits: 4 passes for 32-bit keys,
+//     8 for 64-bit);
+//   * one kernel per digit: tiles of 4096 keys are taken in arrival order
+//     from a flattened (segment, tile) list, ranked per warp with
+//     __match_any_sync (stable: element order within a warp's segment of the
+//     tile, warps in order), their digit counts chained across the segment's
+//     tiles with decoupled look-back (Merrill & Garland 2016), staged
 //     digit-sorted in shared memory and written out in coalesced runs;
-//   * digits where every key falls in one bucket are skipped on the device;
+//   * a digit where all of a segment's keys fall in one bucket is skipped
+//     for that segment on the device;
 //   * the first pass applies the key transform of gpu_sort.rs:1089-1163 to
 //     the raw column and generates the row-index payload; the last pass
 //     writes only the payload (the permutation) to its destination.
+// Many GROUP BY queries finalised together sort as many segments in the
+// same handful of launches.
 #include "radix_sort.cuh"
+
+#include <algorithm>
 
 namespace bolt {
 namespace {
@@ -21,6 +29,7 @@ namespace {
 constexpr int SORT_BLOCK = 256;
 constexpr int SORT_ITEMS = 16;
 constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
+constexpr int HIST_CHUNK = 16384;
 constexpr uint32_t LB_AGG = 1u << 30;
 constexpr uint32_t LB_INC = 2u << 30;
 constexpr uint32_t LB_VAL = (1u << 30) - 1;
@@ -29,6 +38,40 @@ constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
 template <typename K> struct KeyTraits;
 template <> struct KeyTraits<uint32_t> { static constexpr int NPASS = 4; };
 template <> struct KeyTraits<ull> { static constexpr int NPASS = 8; };
+
+struct SegDesc {
+    const void* keys;
+    const uint32_t* payload_in;
+    uint32_t* payload_out;
+    const ull* n_dev;
+    ull n;
+    ull buf_off;
+    uint32_t item_begin;
+    uint32_t hist_begin;
+};
+
+struct SortArgs {
+    int32_t src;
+    int32_t desc;
+    int32_t indirect;
+    int32_t nseg;
+    const SegDesc* segs;
+    const uint32_t* item_begins;  // nseg + 1
+    const uint32_t* hist_begins;  // nseg + 1
+    void* kA;
+    void* kB;
+    uint32_t* pA;
+    uint32_t* pB;
+    uint32_t* hist;        // nseg * NPASS * 256
+    uint32_t* digit_base;  // nseg * NPASS * 256
+    uint32_t* active;      // nseg
+    uint32_t* lookback;    // 2 * lb_stride
+    uint64_t lb_stride;    // total_items * 256
+    uint32_t total_items;
+    uint32_t total_hist_items;
+    uint32_t* tile_ctr;    // NPASS
+    uint32_t* status;
+};
 
 __device__ __forceinline__ uint32_t sort_key_u32(int src, const void* p, uint64_t r, int desc) {
     uint32_t k;
@@ -62,29 +105,6 @@ __device__ __forceinline__ ull load_key<ull>(int src, const void* p, uint64_t r,
     return sort_key_u64(src, p, r, desc);
 }
 
-struct SortArgs {
-    int32_t src;
-    int32_t desc;
-    const void* raw;
-    const uint32_t* payload_in;
-    int32_t indirect;
-    uint64_t n;
-    const ull* n_dev;
-    void* kA;
-    void* kB;
-    uint32_t* pA;
-    uint32_t* pB;
-    uint32_t* payload_out;
-    void* keys_out;
-    uint32_t* hist;        // NPASS * 256
-    uint32_t* digit_base;  // NPASS * 256
-    uint32_t* lookback;    // 2 * lb_stride
-    uint64_t lb_stride;
-    uint32_t* tile_ctr;    // NPASS
-    uint32_t* active;      // 1 word
-    uint32_t* status;
-};
-
 __device__ __forceinline__ void st_volatile_u32(uint32_t* p, uint32_t v) {
     *reinterpret_cast<volatile uint32_t*>(p) = v;
 }
@@ -92,67 +112,90 @@ __device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
     return *reinterpret_cast<const volatile uint32_t*>(p);
 }
 
+// Index of the segment owning flattened item `item` (begins is nondecreasing).
+__device__ __forceinline__ int seg_of(const uint32_t* begins, int nseg, uint32_t item) {
+    int lo = 0, hi = nseg;  // answer in [0, nseg)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(begins + mid) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t seg_n(const SegDesc& d) { return d.n_dev ? *d.n_dev : d.n; }
+
 template <typename K>
 __global__ void __launch_bounds__(256) sort_hist_kernel(SortArgs a) {
     constexpr int NP = KeyTraits<K>::NPASS;
     __shared__ uint32_t h[NP * 256];
-    for (int i = threadIdx.x; i < NP * 256; i += blockDim.x) h[i] = 0;
-    const uint64_t n = a.n_dev ? *a.n_dev : a.n;
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    // Clear the look-back buffer of the first pass and the tile counters.
+    // Clear the first look-back buffer and the pass tile counters.
     for (uint64_t i = tid; i < a.lb_stride; i += stride) a.lookback[i] = 0;
     if (blockIdx.x == 0 && threadIdx.x < NP) a.tile_ctr[threadIdx.x] = 0;
-    __syncthreads();
-    for (uint64_t i = tid; i < n; i += stride) {
-        uint64_t r = a.indirect ? a.payload_in[i] : i;
-        K k = load_key<K>(a.src, a.raw, r, a.desc);
+    for (uint32_t item = blockIdx.x; item < a.total_hist_items; item += gridDim.x) {
+        const int sg = seg_of(a.hist_begins, a.nseg, item);
+        const SegDesc& d = a.segs[sg];
+        const uint64_t n = seg_n(d);
+        const uint64_t c0 = (uint64_t)(item - d.hist_begin) * HIST_CHUNK;
+        for (int i = threadIdx.x; i < NP * 256; i += blockDim.x) h[i] = 0;
+        __syncthreads();
+        const uint64_t c1 = c0 + HIST_CHUNK < n ? c0 + HIST_CHUNK : n;
+        for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+            const uint64_t r = a.indirect ? d.payload_in[i] : i;
+            const K k = load_key<K>(a.src, d.keys, r, a.desc);
 #pragma unroll
-        for (int p = 0; p < NP; ++p) atomicAdd(&h[p * 256 + (uint32_t)((k >> (8 * p)) & 0xFF)], 1u);
+            for (int p = 0; p < NP; ++p) atomicAdd(&h[p * 256 + (uint32_t)((k >> (8 * p)) & 0xFF)], 1u);
+        }
+        __syncthreads();
+        uint32_t* gh = a.hist + (uint64_t)sg * NP * 256;
+        for (int i = threadIdx.x; i < NP * 256; i += blockDim.x)
+            if (h[i]) atomicAdd(&gh[i], h[i]);
+        __syncthreads();
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < NP * 256; i += blockDim.x)
-        if (h[i]) atomicAdd(&a.hist[i], h[i]);
 }
 
-// Exclusive scan of each digit histogram; marks the passes whose digit is
-// not constant over all keys.
+// One CTA per segment: exclusive scan of each digit histogram; marks the
+// passes whose digit is not constant over the segment's keys.
 template <int NP>
 __global__ void __launch_bounds__(256) sort_scan_kernel(SortArgs a) {
     __shared__ uint32_t wsum[8];
     __shared__ uint32_t trivial;
-    const uint64_t n = a.n_dev ? *a.n_dev : a.n;
+    const int sg = blockIdx.x;
+    const uint64_t n = seg_n(a.segs[sg]);
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const uint32_t* hist = a.hist + (uint64_t)sg * NP * 256;
+    uint32_t* base = a.digit_base + (uint64_t)sg * NP * 256;
     uint32_t act = 0;
     for (int p = 0; p < NP; ++p) {
         if (t == 0) trivial = 0;
         __syncthreads();
-        uint32_t v = a.hist[p * 256 + t];
+        const uint32_t v = hist[p * 256 + t];
         if ((uint64_t)v == n) trivial = 1;
         uint32_t x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
         if (lane == 31) wsum[w] = x;
         __syncthreads();
         uint32_t wp = 0;
         for (int i = 0; i < w; ++i) wp += wsum[i];
-        a.digit_base[p * 256 + t] = wp + x - v;
+        base[p * 256 + t] = wp + x - v;
         __syncthreads();
         if (!trivial) act |= 1u << p;
         __syncthreads();
     }
-    if (t == 0) *a.active = act ? act : 1u;
+    if (t == 0) a.active[sg] = act ? act : 1u;
 }
 
 template <typename K>
 __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p) {
     constexpr int NW = SORT_BLOCK / 32;
-    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_item;
     __shared__ uint32_t warp_hist[NW][256];
-    __shared__ uint32_t tile_cnt[256];
     __shared__ uint32_t tile_off[256];
     __shared__ uint32_t gstart[256];
     __shared__ uint32_t wsum[8];
@@ -160,43 +203,45 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
     K* stage_key = reinterpret_cast<K*>(dyn);
     uint32_t* stage_pay = reinterpret_cast<uint32_t*>(dyn + sizeof(K) * SORT_TILE);
 
-    const uint32_t active = *a.active;
+    if (threadIdx.x == 0) s_item = atomicAdd(&a.tile_ctr[p], 1u);
+    for (int i = threadIdx.x; i < NW * 256; i += SORT_BLOCK) (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= a.total_items) return;
+    const int sg = seg_of(a.item_begins, a.nseg, item);
+    const SegDesc& d = a.segs[sg];
+    const uint32_t active = a.active[sg];
     if (!((active >> p) & 1u)) return;
-    const uint64_t n = a.n_dev ? *a.n_dev : a.n;
-    const uint32_t ntiles = (uint32_t)((n + SORT_TILE - 1) / SORT_TILE);
+    const uint64_t n = seg_n(d);
+    const uint32_t tile = item - d.item_begin;
+    if ((uint64_t)tile * SORT_TILE >= n) return;
+
     const uint32_t before = active & ((1u << p) - 1u);
     const bool first = before == 0;
     const bool last = (active >> (p + 1)) == 0;
     const int kidx = __popc(before);
-    const K* kin = (kidx & 1) ? (const K*)a.kA : (const K*)a.kB;
-    const uint32_t* pin = (kidx & 1) ? a.pA : a.pB;
-    K* kout = (kidx & 1) ? (K*)a.kB : (K*)a.kA;
-    uint32_t* pout = last ? a.payload_out : ((kidx & 1) ? a.pB : a.pA);
-    if (last) kout = (K*)a.keys_out;
+    const K* kin = ((kidx & 1) ? (const K*)a.kA : (const K*)a.kB) + d.buf_off;
+    const uint32_t* pin = ((kidx & 1) ? a.pA : a.pB) + d.buf_off;
+    K* kout = last ? nullptr : ((kidx & 1) ? (K*)a.kB : (K*)a.kA) + d.buf_off;
+    uint32_t* pout = last ? d.payload_out : ((kidx & 1) ? a.pB : a.pA) + d.buf_off;
     uint32_t* lb = a.lookback + (uint64_t)(kidx & 1) * a.lb_stride;
     uint32_t* lb_next = a.lookback + (uint64_t)((kidx + 1) & 1) * a.lb_stride;
 
-    if (threadIdx.x == 0) s_tile = atomicAdd(&a.tile_ctr[p], 1u);
-    for (int i = threadIdx.x; i < NW * 256; i += SORT_BLOCK) (&warp_hist[0][0])[i] = 0;
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile >= ntiles) return;
-
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t seg = (uint64_t)tile * SORT_TILE + (uint64_t)w * 32 * SORT_ITEMS;
+    const uint64_t seg0 = (uint64_t)tile * SORT_TILE + (uint64_t)w * 32 * SORT_ITEMS;
     const int shift = 8 * p;
     K key[SORT_ITEMS];
     uint32_t pay[SORT_ITEMS];
     uint32_t rank[SORT_ITEMS];
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
-        uint64_t e = seg + (uint64_t)j * 32 + lane;
+        const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
         key[j] = 0;
         pay[j] = 0;
         if (e < n) {
             if (first) {
-                pay[j] = a.payload_in ? a.payload_in[e] : (uint32_t)e;
-                key[j] = load_key<K>(a.src, a.raw, a.indirect ? pay[j] : e, a.desc);
+                pay[j] = d.payload_in ? d.payload_in[e] : (uint32_t)e;
+                key[j] = load_key<K>(a.src, d.keys, a.indirect ? pay[j] : e, a.desc);
             } else {
                 key[j] = kin[e];
                 pay[j] = pin[e];
@@ -206,48 +251,49 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
     // Stable per-warp ranking in element order.
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
-        uint64_t e = seg + (uint64_t)j * 32 + lane;
-        bool valid = e < n;
-        uint32_t vm = __ballot_sync(0xffffffffu, valid);
+        const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
+        const bool valid = e < n;
+        const uint32_t vm = __ballot_sync(0xffffffffu, valid);
         rank[j] = 0;
         if (valid) {
-            uint32_t d = (uint32_t)(key[j] >> shift) & 0xFFu;
-            uint32_t peers = __match_any_sync(vm, d);
-            int leader = 31 - __clz(peers);
-            uint32_t base = 0;
+            const uint32_t dg = (uint32_t)(key[j] >> shift) & 0xFFu;
+            const uint32_t peers = __match_any_sync(vm, dg);
+            const int leader = 31 - __clz(peers);
+            uint32_t b = 0;
             if (lane == leader) {
-                base = warp_hist[w][d];
-                warp_hist[w][d] = base + __popc(peers);
+                b = warp_hist[w][dg];
+                warp_hist[w][dg] = b + __popc(peers);
             }
-            base = __shfl_sync(vm, base, leader);
-            rank[j] = base + __popc(peers & lanemask_lt());
+            b = __shfl_sync(vm, b, leader);
+            rank[j] = b + __popc(peers & lanemask_lt());
         }
         __syncwarp();
     }
     __syncthreads();
 
-    // Per-digit warp offsets, tile counts, and the cross-tile look-back.
+    // Per-digit warp offsets, tile counts, and the look-back over the
+    // segment's earlier tiles.
     {
-        const uint32_t d = threadIdx.x;  // SORT_BLOCK == 256
+        const uint32_t dg = threadIdx.x;  // SORT_BLOCK == 256
         uint32_t run = 0;
 #pragma unroll
         for (int ww = 0; ww < NW; ++ww) {
-            uint32_t c = warp_hist[ww][d];
-            warp_hist[ww][d] = run;
+            const uint32_t c = warp_hist[ww][dg];
+            warp_hist[ww][dg] = run;
             run += c;
         }
-        tile_cnt[d] = run;
-        uint32_t* my = lb + (uint64_t)tile * 256 + d;
+        uint32_t* my = lb + (uint64_t)item * 256 + dg;
         uint32_t excl = 0;
         if (tile == 0) {
             st_volatile_u32(my, LB_INC | run);
         } else {
             st_volatile_u32(my, LB_AGG | run);
-            int64_t t = (int64_t)tile - 1;
+            int64_t t = (int64_t)item - 1;
+            const int64_t t_end = (int64_t)d.item_begin;
             uint32_t spins = 0;
-            while (t >= 0) {
-                uint32_t v = ld_volatile_u32(lb + (uint64_t)t * 256 + d);
-                uint32_t st = v >> 30;
+            while (t >= t_end) {
+                const uint32_t v = ld_volatile_u32(lb + (uint64_t)t * 256 + dg);
+                const uint32_t st = v >> 30;
                 if (st == 0) {
                     if (++spins > LB_SPIN_LIMIT) {
                         atomicOr(a.status, ST_FLAG_TIMEOUT);
@@ -262,30 +308,30 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
             }
             st_volatile_u32(my, LB_INC | ((excl + run) & LB_VAL));
         }
-        lb_next[(uint64_t)tile * 256 + d] = 0;
-        gstart[d] = a.digit_base[p * 256 + d] + excl;
+        lb_next[(uint64_t)item * 256 + dg] = 0;
+        gstart[dg] = a.digit_base[((uint64_t)sg * KeyTraits<K>::NPASS + p) * 256 + dg] + excl;
         // Exclusive scan of the tile's digit counts.
         uint32_t x = run;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
         if (lane == 31) wsum[w] = x;
         __syncthreads();
         uint32_t wp = 0;
         for (int i = 0; i < w; ++i) wp += wsum[i];
-        tile_off[d] = wp + x - run;
+        tile_off[dg] = wp + x - run;
     }
     __syncthreads();
 
     // Stage digit-sorted, then write coalesced runs.
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
-        uint64_t e = seg + (uint64_t)j * 32 + lane;
+        const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
         if (e < n) {
-            uint32_t d = (uint32_t)(key[j] >> shift) & 0xFFu;
-            uint32_t pos = tile_off[d] + warp_hist[w][d] + rank[j];
+            const uint32_t dg = (uint32_t)(key[j] >> shift) & 0xFFu;
+            const uint32_t pos = tile_off[dg] + warp_hist[w][dg] + rank[j];
             stage_key[pos] = key[j];
             stage_pay[pos] = pay[j];
         }
@@ -294,9 +340,9 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
     const uint64_t tb = (uint64_t)tile * SORT_TILE;
     const uint32_t tile_n = (uint32_t)((n - tb) < (uint64_t)SORT_TILE ? (n - tb) : (uint64_t)SORT_TILE);
     for (uint32_t i = threadIdx.x; i < tile_n; i += SORT_BLOCK) {
-        K k = stage_key[i];
-        uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
-        uint64_t g = (uint64_t)gstart[d] + (i - tile_off[d]);
+        const K k = stage_key[i];
+        const uint32_t dg = (uint32_t)(k >> shift) & 0xFFu;
+        const uint64_t g = (uint64_t)gstart[dg] + (i - tile_off[dg]);
         if (g >= n) {  // only reachable after a look-back timeout
             atomicOr(a.status, ST_FLAG_TIMEOUT);
             continue;
@@ -309,44 +355,68 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
 template <typename K>
 bolt_status run_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
     constexpr int NP = KeyTraits<K>::NPASS;
-    const uint64_t n = sp.n;
-    if (n >= (1ull << 30)) return fail(ctx, BOLT_DECLINE, "radix sort: %llu rows exceed the 2^30 row limit", (ull)n);
-    const uint64_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
-    const uint64_t nb = n ? n : 1;
+    const int nseg = (int)sp.segs.size();
+    if (nseg == 0) return BOLT_OK;
+    std::vector<SegDesc> segs(nseg);
+    std::vector<uint32_t> begins(2 * (nseg + 1));
+    uint64_t total_n = 0, items = 0, hitems = 0;
+    for (int i = 0; i < nseg; ++i) {
+        const SortSegment& g = sp.segs[i];
+        if (g.n >= (1ull << 30))
+            return fail(ctx, BOLT_DECLINE, "radix sort: %llu rows exceed the 2^30 row limit", (ull)g.n);
+        if (!g.payload_out && g.n) return fail(ctx, BOLT_ERR_INVALID, "radix sort: no payload output");
+        segs[i] = SegDesc{g.keys, g.payload_in, g.payload_out, g.n_dev, g.n, total_n, (uint32_t)items, (uint32_t)hitems};
+        begins[i] = (uint32_t)items;
+        begins[nseg + 1 + i] = (uint32_t)hitems;
+        total_n += g.n;
+        items += (g.n + SORT_TILE - 1) / SORT_TILE;
+        hitems += (g.n + HIST_CHUNK - 1) / HIST_CHUNK;
+    }
+    begins[nseg] = (uint32_t)items;
+    begins[2 * nseg + 1] = (uint32_t)hitems;
+    if (items >= (1ull << 31)) return fail(ctx, BOLT_DECLINE, "radix sort: too many tiles");
+    if (items == 0) return BOLT_OK;
+
     SortArgs a{};
     a.src = sp.src;
     a.desc = sp.descending;
-    a.raw = sp.keys;
-    a.payload_in = sp.payload_in;
     a.indirect = sp.indirect;
-    a.n = n;
-    a.n_dev = sp.n_dev;
+    a.nseg = nseg;
+    a.total_items = (uint32_t)items;
+    a.total_hist_items = (uint32_t)hitems;
+    a.lb_stride = items * 256;
+    const uint64_t nb = total_n ? total_n : 1;
+    SegDesc* d_segs = (SegDesc*)arena_alloc(ctx, sizeof(SegDesc) * nseg);
+    uint32_t* d_begins = (uint32_t*)arena_alloc(ctx, 4 * begins.size());
     a.kA = arena_alloc(ctx, nb * sizeof(K));
     a.kB = arena_alloc(ctx, nb * sizeof(K));
     a.pA = (uint32_t*)arena_alloc(ctx, nb * 4);
     a.pB = (uint32_t*)arena_alloc(ctx, nb * 4);
-    a.hist = (uint32_t*)arena_alloc(ctx, NP * 256 * 4);
-    a.digit_base = (uint32_t*)arena_alloc(ctx, NP * 256 * 4);
-    a.lb_stride = (ntiles ? ntiles : 1) * 256;
+    a.hist = (uint32_t*)arena_alloc(ctx, (uint64_t)nseg * NP * 256 * 4);
+    a.digit_base = (uint32_t*)arena_alloc(ctx, (uint64_t)nseg * NP * 256 * 4);
+    a.active = (uint32_t*)arena_alloc(ctx, (uint64_t)nseg * 4);
     a.lookback = (uint32_t*)arena_alloc(ctx, 2 * a.lb_stride * 4);
     a.tile_ctr = (uint32_t*)arena_alloc(ctx, 64);
-    a.active = (uint32_t*)arena_alloc(ctx, 64);
     a.status = ctx->d_status;
-    a.payload_out = sp.payload_out;
-    a.keys_out = sp.keys_out;
-    if (!a.kA || !a.kB || !a.pA || !a.pB || !a.hist || !a.digit_base || !a.lookback || !a.tile_ctr || !a.active)
-        return fail(ctx, BOLT_ERR_CAPACITY, "radix sort: scratch arena too small for %llu rows", (ull)n);
-
-    BOLT_CUDA(ctx, cudaMemsetAsync(a.hist, 0, NP * 256 * 4, s));
-    unsigned hb = grid_for(n, 256 * 8, (unsigned)ctx->num_sms * 8);
+    if (!d_segs || !d_begins || !a.kA || !a.kB || !a.pA || !a.pB || !a.hist || !a.digit_base || !a.active ||
+        !a.lookback || !a.tile_ctr)
+        return fail(ctx, BOLT_ERR_CAPACITY, "radix sort: scratch arena too small for %llu rows", (ull)total_n);
+    a.segs = d_segs;
+    a.item_begins = d_begins;
+    a.hist_begins = d_begins + nseg + 1;
+    bolt_status st = stage_upload(ctx, s, d_segs, segs.data(), sizeof(SegDesc) * nseg);
+    if (st != BOLT_OK) return st;
+    st = stage_upload(ctx, s, d_begins, begins.data(), 4 * begins.size());
+    if (st != BOLT_OK) return st;
+    BOLT_CUDA(ctx, cudaMemsetAsync(a.hist, 0, (uint64_t)nseg * NP * 256 * 4, s));
+    const unsigned hb = (unsigned)std::min<uint64_t>(hitems, (uint64_t)ctx->num_sms * 8);
     sort_hist_kernel<K><<<hb, 256, 0, s>>>(a);
-    sort_scan_kernel<NP><<<1, 256, 0, s>>>(a);
+    sort_scan_kernel<NP><<<nseg, 256, 0, s>>>(a);
     ctx->last_launches += 2;
     const size_t dyn = (sizeof(K) + 4) * SORT_TILE;
     BOLT_CUDA(ctx, cudaFuncSetAttribute(sort_pass_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    const unsigned grid = (unsigned)(ntiles ? ntiles : 1);
     for (int p = 0; p < NP; ++p) {
-        sort_pass_kernel<K><<<grid, SORT_BLOCK, dyn, s>>>(a, p);
+        sort_pass_kernel<K><<<(unsigned)items, SORT_BLOCK, dyn, s>>>(a, p);
         ctx->last_launches++;
     }
     BOLT_CUDA(ctx, cudaGetLastError());
@@ -355,14 +425,13 @@ bolt_status run_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
 
 }  // namespace
 
-uint64_t radix_sort_scratch(uint64_t n, int32_t src) {
+uint64_t radix_sort_scratch(uint64_t total_n, uint64_t nseg, int32_t src) {
     const uint64_t ksz = (src == SRC_I32 || src == SRC_F32 || src == SRC_U32) ? 4 : 8;
-    const uint64_t ntiles = (n + SORT_TILE - 1) / SORT_TILE + 1;
-    return 2 * n * ksz + 2 * n * 4 + 2 * ntiles * 256 * 4 + 8 * 256 * 8 + 16 * 256;
+    const uint64_t items = total_n / SORT_TILE + nseg + 1;
+    return 2 * total_n * (ksz + 4) + 2 * items * 256 * 4 + nseg * (2 * 8 * 256 * 4 + 96) + 64 * 1024;
 }
 
 bolt_status radix_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
-    if (!sp.payload_out) return fail(ctx, BOLT_ERR_INVALID, "radix sort: no payload output");
     switch (sp.src) {
     case SRC_I32:
     case SRC_F32:
@@ -423,19 +492,22 @@ extern "C" bolt_status bolt_radix_sort_perm_multi(bolt_ctx* ctx, const bolt_col_
     ull* cnt = (ull*)arena_alloc(ctx, 256);
     if ((n_keys > 1 && !tmp) || !cnt) return fail(ctx, BOLT_ERR_CAPACITY, "ORDER BY: scratch arena too small");
     const uint32_t* cur = nullptr;  // nullptr = identity order
+    kernel_mark_begin(ctx, flags, s);
     for (int k = n_keys - 1; k >= 0; --k) {
         uint32_t* dst = ((n_keys - 1 - k) % 2 == (n_keys - 1) % 2) ? out : tmp;
         const uint64_t mark = ctx->arena_used;
         const bolt_col_view& key = keys[k];
         SortSpec sp;
         sp.src = sort_src_of(key.dtype);
-        sp.keys = key.data;
         sp.descending = descending[k];
+        SortSegment seg;
+        seg.keys = key.data;
         if (!key.validity) {
-            sp.payload_in = cur;
+            seg.payload_in = cur;
             sp.indirect = cur != nullptr;
-            sp.n = n;
-            sp.payload_out = dst;
+            seg.n = n;
+            seg.payload_out = dst;
+            sp.segs.push_back(seg);
             st = radix_sort(ctx, s, sp);
             if (st != BOLT_OK) return st;
         } else {
@@ -451,26 +523,27 @@ extern "C" bolt_status bolt_radix_sort_perm_multi(bolt_ctx* ctx, const bolt_col_
             cv.n_out_dev = cnt;
             st = compact_enqueue(ctx, s, cv);
             if (st != BOLT_OK) return st;
-            ull nv = 0;
             BOLT_CUDA(ctx, cudaMemcpyAsync(ctx->h_words, cnt, 8, cudaMemcpyDeviceToHost, s));
             BOLT_CUDA(ctx, cudaStreamSynchronize(s));
-            nv = ctx->h_words[0];
+            const ull nv = ctx->h_words[0];
             const uint64_t nn = n - nv;
             CompactSpec cn = cv;
             cn.invert = 1;
             cn.row_ids = dst + (nulls_first[k] ? 0 : nv);
             st = compact_enqueue(ctx, s, cn);
             if (st != BOLT_OK) return st;
-            sp.payload_in = valid_ids;
+            seg.payload_in = valid_ids;
             sp.indirect = 1;
-            sp.n = nv;
-            sp.payload_out = dst + (nulls_first[k] ? nn : 0);
+            seg.n = nv;
+            seg.payload_out = dst + (nulls_first[k] ? nn : 0);
+            sp.segs.push_back(seg);
             st = radix_sort(ctx, s, sp);
             if (st != BOLT_OK) return st;
         }
         ctx->arena_used = mark;
         cur = dst;
     }
+    kernel_mark_end(ctx, flags, s);
     st = call_end(ctx, flags, s);
     if (st != BOLT_OK) return st;
     if (flags & BOLT_FLAG_ASYNC) return BOLT_OK;

@@ -1,5 +1,8 @@
-// radix_sort.cuh — onesweep LSD radix sort (8-bit digits, decoupled look-back).
+// radix_sort.cuh — onesweep LSD radix sort (8-bit digits, decoupled look-back)
+// over one or many independent segments in the same launches.
 #pragma once
+
+#include <vector>
 
 #include "ctx.cuh"
 
@@ -15,24 +18,27 @@ enum SortSrc : int32_t {
     SRC_U32 = 5,
 };
 
-struct SortSpec {
-    int32_t src = SRC_U64_KEYS;
-    const void* keys = nullptr;         // raw column or u64 keys
-    int32_t descending = 0;
-    // Payload input: nullptr = row index (iota). When `indirect` is set the
-    // keys are read as keys[payload_in[i]] (multi-key / NULL-partitioned sorts).
+// One independent sort. Payload input nullptr = row index (iota). With
+// `indirect` (a spec-wide flag) keys are read as keys[payload_in[i]].
+struct SortSegment {
+    const void* keys = nullptr;
     const uint32_t* payload_in = nullptr;
-    int32_t indirect = 0;
-    uint64_t n = 0;                      // host row count (upper bound when n_dev is set)
-    const ull* n_dev = nullptr;          // optional device row count
-    uint32_t* payload_out = nullptr;     // sorted payload (required)
-    ull* keys_out = nullptr;             // optional sorted u64 keys (SRC_U64_KEYS only)
+    uint32_t* payload_out = nullptr;   // sorted payload (required)
+    const ull* n_dev = nullptr;        // optional device row count (n is then an upper bound)
+    uint64_t n = 0;
 };
 
-// Enqueues the sort on `s`. Scratch comes from the context arena.
+struct SortSpec {
+    int32_t src = SRC_U64_KEYS;
+    int32_t descending = 0;
+    int32_t indirect = 0;
+    std::vector<SortSegment> segs;
+};
+
+// Enqueues the sort of every segment on `s`. Scratch comes from the arena.
 bolt_status radix_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& spec);
 
-// Scratch bytes radix_sort needs for n rows of the given source.
-uint64_t radix_sort_scratch(uint64_t n, int32_t src);
+// Scratch bytes radix_sort needs for segments of the given sizes.
+uint64_t radix_sort_scratch(uint64_t total_n, uint64_t nseg, int32_t src);
 
 }  // namespace bolt

@@ -1,0 +1,103 @@
+"""GPU parity: hash join build/probe and the fused join -> GROUP BY against
+the oracle (bit-exact pairs in probe order, exact Decimal128 sums)."""
+
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+
+from helpers import bitmap, golden, spec_arrays
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", golden()["join"], ids=lambda c: c["name"])
+def test_join_known_answers(bolt, engine, oracle, case):
+    bd, bv, bdt, _ = spec_arrays(case["build"])
+    pd, pv, pdt, _ = spec_arrays(case["probe"])
+    r = engine.hash_join_indices(bolt.col(bd, bdt, bv).to("cuda"), bolt.col(pd, pdt, pv).to("cuda"))
+    pr, br = (x.cpu().numpy().view(np.uint32) for x in r)
+    assert len(pr) == case["expected"]["n_pairs"]
+    wp, wb = oracle.hash_join(oracle.HostCol(bd, bdt, bv), oracle.HostCol(pd, pdt, pv))
+    assert np.array_equal(pr, wp) and np.array_equal(br, wb)
+
+
+@pytest.mark.parametrize("dt", ["i32", "i64"])
+def test_join_random_with_nulls(bolt, engine, oracle, dt):
+    rng = np.random.default_rng(31)
+    nb, npr = 50_000, 400_000
+    bk = rng.permutation(1_000_000)[:nb].astype(np.int64) - 500_000
+    if dt == "i64":
+        bk = bk * 1_000_003
+    pk = np.where(rng.random(npr) < 0.7, bk[rng.integers(0, nb, npr)], rng.integers(-2**40, 2**40, npr))
+    bk = bk.astype(np.int32 if dt == "i32" else np.int64)
+    pk = pk.astype(np.int32 if dt == "i32" else np.int64)
+    bvalid = rng.random(nb) > 0.05
+    pvalid = rng.random(npr) > 0.05
+    b = bolt.col(bk, dt, bitmap(bvalid)).to("cuda")
+    p = bolt.col(pk, dt, bitmap(pvalid)).to("cuda")
+    pr, br = (x.cpu().numpy().view(np.uint32) for x in engine.hash_join_indices(b, p))
+    wp, wb = oracle.hash_join(oracle.HostCol(bk, dt, bitmap(bvalid)), oracle.HostCol(pk, dt, bitmap(pvalid)))
+    assert np.array_equal(pr, wp) and np.array_equal(br, wb)
+
+
+def test_join_key_minus_one_and_duplicates(bolt, engine, oracle):
+    b = np.array([-1, 4, 9], np.int64)
+    p = np.array([9, -1, 3, -1, 4], np.int64)
+    pr, br = (x.cpu().numpy().view(np.uint32) for x in
+              engine.hash_join_indices(bolt.col(b, "i64").to("cuda"), bolt.col(p, "i64").to("cuda")))
+    assert pr.tolist() == [0, 1, 3, 4] and br.tolist() == [2, 0, 0, 1]
+    dup = np.array([1, 2, 1], np.int64)
+    assert engine.hash_join_indices(bolt.col(dup, "i64").to("cuda"), bolt.col(p, "i64").to("cuda")) is None
+
+
+def test_join_capacity_error(bolt, engine, oracle):
+    b = np.arange(100, dtype=np.int64)
+    p = np.tile(b, 10)
+    with pytest.raises(bolt.GpuCapacityError):
+        engine.hash_join_indices(bolt.col(b, "i64").to("cuda"), bolt.col(p, "i64").to("cuda"), out_cap=50)
+
+
+@pytest.mark.parametrize("nb,npr", [(10_000, 200_000), (1_000_000, 4_000_000)])
+def test_join_groupby_decimal(bolt, engine, oracle, nb, npr):
+    """SELECT b.g, SUM(p.amount), COUNT(*) FROM p JOIN b ON p.fk = b.k GROUP BY b.g."""
+    dg = importlib.import_module("craton_bolt_b200.datagen")
+    bt = dg.join_build(nb, seed=3)
+    pt = dg.join_probe(npr, nb, seed=3)
+    g, s, c = engine.join_groupby(bolt.col(bt["k"], "i64").to("cuda"), bolt.col(bt["g"], "i32").to("cuda"),
+                                  bolt.col(pt["fk"], "i64").to("cuda"),
+                                  bolt.col(pt["amount"], "dec128", scale=2).to("cuda"))
+    wg, wlo, whi, wc = oracle.join_groupby(oracle.HostCol(bt["k"], "i64"), bt["g"], oracle.HostCol(pt["fk"], "i64"),
+                                           oracle.HostCol(pt["amount"], "dec128", scale=2))
+    assert np.array_equal(g.numpy(), wg)
+    sd = s.numpy()
+    assert np.array_equal(sd[:, 0], wlo) and np.array_equal(sd[:, 1], whi)
+    assert np.array_equal(c.numpy(), wc)
+    assert s.scale == 2
+
+
+def test_join_groupby_wide_decimal_and_overflow(bolt, engine, oracle):
+    bk = np.arange(4, dtype=np.int64)
+    bg = np.array([0, 1, 0, 1], np.int32)
+    pk = np.array([0, 1, 2, 3, 0], np.int64)
+    big = 10**30
+    vals = [big, -5, big, 7, -3]
+    lo = np.array([v & (2**64 - 1) for v in vals], np.uint64).view(np.int64)
+    hi = np.array([(v >> 64) & (2**64 - 1) for v in vals], np.uint64).view(np.int64)
+    amt = np.stack([lo, hi], axis=1)
+    g, s, c = engine.join_groupby(bolt.col(bk, "i64").to("cuda"), bolt.col(bg, "i32").to("cuda"),
+                                  bolt.col(pk, "i64").to("cuda"), bolt.col(amt, "dec128").to("cuda"))
+    sd = s.numpy()
+    got = [(int(h) << 64) | (int(l) & (2**64 - 1)) for l, h in sd]
+    assert g.numpy().tolist() == [0, 1]
+    assert got == [2 * big - 3, 2]
+    assert c.numpy().tolist() == [3, 2]
+    huge = 10**38 - 1
+    lo = np.array([huge & (2**64 - 1)] * 2, np.uint64).view(np.int64)
+    hi = np.array([huge >> 64] * 2, np.uint64).view(np.int64)
+    with pytest.raises(bolt.TypeError_):
+        engine.join_groupby(bolt.col(bk[:2], "i64").to("cuda"), bolt.col(np.zeros(2, np.int32), "i32").to("cuda"),
+                            bolt.col(np.array([0, 1], np.int64), "i64").to("cuda"),
+                            bolt.col(np.stack([lo, hi], axis=1), "dec128").to("cuda"))
