@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 from . import _abi
-from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLOBAL, FLAG_FORCE_SHMEM,
+from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLOBAL, FLAG_FORCE_SHMEM, FLAG_NO_TUNE,
                    FLAG_PROFILE)
 
 __all__ = ["BoltError", "DeclineError", "SpillError", "TypeError_", "GpuCapacityError", "TimeoutError_",
@@ -287,6 +287,24 @@ class Engine:
         if r is None:
             raise DeclineError(f"GROUP BY declined: {self._lib.bolt_ctx_last_error(self._ctx).decode()}")
         return r
+
+    def autotune_groupby(self, pq: "PreparedGroupby") -> float:
+        """Times candidate launch choices for this query shape on the device
+        and keeps the fastest in the context (bolt_groupby_autotune).
+        Returns the winner's device milliseconds."""
+        best = C.c_double(0.0)
+        st = self._lib.bolt_groupby_autotune(self._ctx, C.byref(pq.desc), C.byref(pq.out),
+                                             C.c_void_p(self.stream_handle), C.byref(best))
+        self._check(st, "GROUP BY autotune")
+        return float(best.value)
+
+    def save_tuning(self, path: str):
+        if self._lib.bolt_ctx_tuning_save(self._ctx, str(path).encode()) != _abi.OK:
+            raise PlanError(f"cannot write tuning file {path}")
+
+    def load_tuning(self, path: str):
+        st = self._lib.bolt_ctx_tuning_load(self._ctx, str(path).encode())
+        self._check(st, "load tuning")
 
     def execute_batch(self, prepared: Sequence["PreparedGroupby"], flags: int = 0) -> list[GroupbyResult]:
         """Runs many prepared GROUP BY queries as one batch (one persistent

@@ -34,6 +34,7 @@ FLAG_ASYNC = 0x1
 FLAG_PROFILE = 0x2
 FLAG_FORCE_GLOBAL = 0x4
 FLAG_FORCE_SHMEM = 0x8
+FLAG_NO_TUNE = 0x10
 
 
 class ColView(C.Structure):
@@ -90,6 +91,10 @@ SIGNATURES = {
     "bolt_ctx_scratch_bytes": (C.c_uint64, [C.c_void_p]),
     "bolt_version": (C.c_char_p, []),
     "bolt_groupby": (C.c_int, [C.c_void_p, C.POINTER(GroupbyDesc), C.POINTER(GroupbyOut), C.c_uint32, C.c_void_p]),
+    "bolt_groupby_autotune": (C.c_int, [C.c_void_p, C.POINTER(GroupbyDesc), C.POINTER(GroupbyOut), C.c_void_p,
+                                        C.POINTER(C.c_double)]),
+    "bolt_ctx_tuning_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "bolt_ctx_tuning_load": (C.c_int, [C.c_void_p, C.c_char_p]),
     "bolt_hash_join_build": (C.c_int, [C.c_void_p, C.POINTER(ColView), C.POINTER(ColView), C.c_uint32,
                                        C.c_void_p, C.POINTER(C.c_void_p)]),
     "bolt_hash_join_probe": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(ColView), C.POINTER(ColMut),
@@ -109,6 +114,10 @@ SIGNATURES = {
                                     C.POINTER(ColMut), C.POINTER(C.c_uint64), C.c_uint32, C.c_void_p]),
     "bolt_batch_groupby": (C.c_int, [C.c_void_p, C.POINTER(Query), C.c_int32, C.c_uint32, C.c_void_p]),
     "bolt_groupby_footprint": (C.c_uint64, [C.POINTER(GroupbyDesc), C.c_uint64]),
+    "bolt_batch_graph_create": (C.c_int, [C.c_int, C.POINTER(Query), C.c_int32, C.POINTER(C.c_void_p)]),
+    "bolt_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bolt_graph_sync_status": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
+    "bolt_graph_destroy": (None, [C.c_void_p]),
     "bolt_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "bolt_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
     "bolt_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_double)]),

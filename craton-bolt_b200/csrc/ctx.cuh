@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 
 #include "common.cuh"
 
@@ -44,6 +45,9 @@ struct bolt_ctx {
     struct StageUse { uint64_t off, len; cudaEvent_t ev; bool live; };
     StageUse stage_use[STAGE_SLOTS] = {};
     uint32_t stage_next = 0;
+    // Autotuned GROUP BY launch choices per query shape (see gb_shape_key).
+    struct GbTune { int32_t block, smem_shift, warp_agg, load_shift; double ms; };
+    std::unordered_map<uint64_t, GbTune> tune;
 };
 
 namespace bolt {

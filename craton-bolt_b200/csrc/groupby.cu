@@ -764,9 +764,25 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
 // ---------------------------------------------------------------------------
 // Planning
 // ---------------------------------------------------------------------------
+uint64_t gb_shape_key(const GbParams& p, uint64_t n_rows, uint64_t groups_hint) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        h ^= v;
+        h *= 1099511628211ull;
+    };
+    mix((uint64_t)p.n_keys);
+    for (int k = 0; k < p.n_keys; ++k) mix((uint64_t)p.kdtype[k]);
+    mix((uint64_t)p.n_pred);
+    mix(p.jslots ? 1 : 0);
+    for (int s = 0; s < p.n_st; ++s) mix(((uint64_t)p.st[s].kind << 8) | (uint64_t)p.st[s].dtype);
+    mix((uint64_t)ceil_log2_u64(n_rows + 1));
+    mix((uint64_t)ceil_log2_u64(groups_hint + 1));
+    return h;
+}
+
 bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupby_out* out,
                     uint64_t row_begin, uint64_t row_end, uint32_t flags, int mode,
-                    uint64_t cap_override, GbPlan* pl) {
+                    uint64_t cap_override, GbPlan* pl, const bolt_ctx::GbTune* force_tune) {
     if (!d || !out || !d->cols || d->n_cols <= 0) return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: missing table");
     if (d->n_keys < 1 || d->n_keys > 2 || !d->key_cols)
         return fail(ctx, BOLT_DECLINE, "GROUP BY: %d key columns (1 or 2 supported)", d->n_keys);
@@ -906,10 +922,22 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     for (int a = 0; a < d->n_aggs; ++a) out_cap = std::min<uint64_t>(out_cap, out->aggs[a].cap);
     f.out_cap = out_cap;
 
-    // Table sizing: 2x the expected groups (load <= 0.5), grown on demand.
+    // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
+    pl->shape = gb_shape_key(p, n, d->groups_hint);
+    bolt_ctx::GbTune tn{512, 0, 0, 1, 0.0};
+    if (!(flags & BOLT_FLAG_NO_TUNE)) {
+        auto it = ctx->tune.find(pl->shape);
+        if (it != ctx->tune.end()) tn = it->second;
+    }
+    if (force_tune) tn = *force_tune;
+    pl->tune = tn;
+
+    // Table sizing: (2 << load_shift - 1)x the expected groups (default 2x,
+    // load <= 0.5), grown on demand.
     uint64_t cap;
     if (cap_override) cap = cap_override;
-    else if (d->groups_hint) cap = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * d->groups_hint + 16, 64));
+    else if (d->groups_hint)
+        cap = 1ull << ceil_log2_u64(std::max<uint64_t>((d->groups_hint << tn.load_shift) + 16, 64));
     else cap = 1ull << ceil_log2_u64(std::max<uint64_t>(std::min<uint64_t>(2 * n + 16, 1ull << 16), 64));
     pl->cap = cap;
     p.log2cap = f.log2cap = ceil_log2_u64(cap);
@@ -919,7 +947,9 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     p.n_rows = n;
     p.fx_e = 126 - 32 - ceil_log2_u64(n + 1);
     f.fx_e = p.fx_e;
-    p.warp_agg = 0;
+    p.warp_agg = tn.warp_agg;
+    for (int s = 0; s < n_st; ++s)
+        if (p.st[s].kind == K_SUM_D128) p.warp_agg = 0;  // D128 partials do not combine in registers
 
     // Shared-memory tier: the largest power of two of slots that fits the
     // opt-in limit, no larger than 2x the expected groups.
@@ -931,11 +961,13 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         const uint64_t want = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * (d->groups_hint ? d->groups_hint : cap), 256));
         while (sl > 8 && (1ull << sl) > want) --sl;
         if (((size_t)1 << sl) * entry > budget) sl = 0;
+        if (tn.smem_shift >= 8) sl = 0;
+        else if (sl) sl = std::max(sl - tn.smem_shift, 6);
     }
     p.smem_log2 = sl;
     pl->smem_entries = sl ? (1 << sl) : 0;
     pl->u = n_st <= 4 ? 4 : 2;
-    pl->block = 512;
+    pl->block = tn.block;
     pl->small_final = cap <= SMALL_FINAL_MAX;
     p.status = ctx->d_status;
     f.status = ctx->d_status;
@@ -1301,6 +1333,90 @@ extern "C" bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* qs, int32_t
     for (int i = 0; i < n; ++i)
         if (qs[i].status != BOLT_OK)
             return fail(ctx, qs[i].status, "batched GROUP BY: query %d failed (%s)", i, bolt_status_str(qs[i].status));
+    return BOLT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner
+// ---------------------------------------------------------------------------
+extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_desc* desc, bolt_groupby_out* out,
+                                             bolt_stream stream, double* best_ms) {
+    if (!ctx || !desc || !out) return BOLT_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint64_t nrows = 0;
+    if (desc->n_keys >= 1 && desc->key_cols && desc->cols && desc->key_cols[0] >= 0 && desc->key_cols[0] < desc->n_cols)
+        nrows = desc->cols[desc->key_cols[0]].len;
+    // A plain run first: it settles the table size and accumulator modes.
+    bolt_status st = gb_single(ctx, desc, out, 0, nrows, BOLT_FLAG_NO_TUNE, s, nullptr, nullptr, "GROUP BY autotune");
+    if (st != BOLT_OK) return st;
+    std::vector<bolt_ctx::GbTune> cands;
+    for (int block : {256, 512})
+        for (int smem_shift : {0, 1, 2, 8})
+            for (int warp_agg : {0, 1})
+                for (int load_shift : {1, 2}) cands.push_back({block, smem_shift, warp_agg, load_shift, 0.0});
+    bolt_ctx::GbTune best{512, 0, 0, 1, 1e30};
+    uint64_t shape = 0;
+    for (auto& c : cands) {
+        double tot = 0.0;
+        bool ok = true;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+            st = call_begin(ctx, 0, s);
+            if (st != BOLT_OK) return st;
+            GbPlan pl;
+            st = gb_plan(ctx, desc, out, 0, nrows, 0, 0, 0, &pl, &c);
+            if (st != BOLT_OK) return st;
+            shape = pl.shape;
+            BOLT_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+            GbPlan* one = &pl;
+            st = gb_run(ctx, &one, 1, s, 0);
+            if (st != BOLT_OK) return st;
+            BOLT_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+            uint32_t f = 0;
+            st = read_status(ctx, s, 0, &f);
+            if (st != BOLT_OK) return st;
+            if (f) {
+                ok = false;  // this candidate spilled / flagged: not eligible
+                break;
+            }
+            float ms = 0.f;
+            BOLT_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            if (rep > 0) tot += ms;  // first repetition warms up
+        }
+        if (ok && tot / 2 < best.ms) {
+            best = c;
+            best.ms = tot / 2;
+        }
+    }
+    if (best.ms < 1e29) ctx->tune[shape] = best;
+    if (best_ms) *best_ms = best.ms;
+    // Leave `out` holding the result of the tuned configuration.
+    return gb_single(ctx, desc, out, 0, nrows, 0, s, nullptr, nullptr, "GROUP BY autotune");
+}
+
+extern "C" bolt_status bolt_ctx_tuning_save(const bolt_ctx* ctx, const char* path) {
+    if (!ctx || !path) return BOLT_ERR_INVALID;
+    FILE* fp = std::fopen(path, "w");
+    if (!fp) return BOLT_ERR_INVALID;
+    for (const auto& kv : ctx->tune)
+        std::fprintf(fp, "%llx %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
+                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.ms);
+    std::fclose(fp);
+    return BOLT_OK;
+}
+
+extern "C" bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path) {
+    if (!ctx || !path) return BOLT_ERR_INVALID;
+    FILE* fp = std::fopen(path, "r");
+    if (!fp) return fail(ctx, BOLT_ERR_INVALID, "tuning file %s not readable", path);
+    unsigned long long key;
+    bolt_ctx::GbTune t{};
+    while (std::fscanf(fp, "%llx %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift, &t.ms) == 6) {
+        const bool valid = (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
+                           t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 1 &&
+                           t.load_shift <= 3;
+        if (valid) ctx->tune[(uint64_t)key] = t;
+    }
+    std::fclose(fp);
     return BOLT_OK;
 }
 

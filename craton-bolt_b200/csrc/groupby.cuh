@@ -123,16 +123,23 @@ struct GbPlan {
     int32_t mode = 0;
     uint32_t flags = 0;
     ull* words = nullptr;  // device: [0] occupancy, [1] non-NULL groups, [2] groups, [3] status
+    uint64_t shape = 0;    // autotuning key of the query shape
+    bolt_ctx::GbTune tune{512, 0, 0, 1, 0.0};
 };
+
+// Key of a query shape for the autotuning cache: key / predicate / state
+// layout plus the row and group counts rounded to powers of two.
+uint64_t gb_shape_key(const GbParams& p, uint64_t n_rows, uint64_t groups_hint);
 
 // Plan modes selected after a flagged first attempt.
 constexpr int GB_MODE_F64_ATOMIC = 1;  // f64 SUM with plain atomics (non-finite / huge inputs)
 constexpr int GB_MODE_WIDE_DEC = 2;    // Decimal128 SUM with the exact 192-bit state
 
 // Builds the plan for `desc` over rows [row_begin, row_end) (no device work).
+// `force_tune` (nullable) overrides the context's tuning cache.
 bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* desc, const bolt_groupby_out* out,
                     uint64_t row_begin, uint64_t row_end, uint32_t flags, int mode,
-                    uint64_t cap_override, GbPlan* plan);
+                    uint64_t cap_override, GbPlan* plan, const bolt_ctx::GbTune* force_tune = nullptr);
 
 // Bytes of scratch the plan needs (table + finalize buffers).
 uint64_t gb_plan_scratch(const GbPlan& plan);

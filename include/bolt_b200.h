@@ -89,6 +89,7 @@ typedef struct bolt_ctx bolt_ctx;
 #define BOLT_FLAG_PROFILE      0x2u  /* record device time of the call (bolt_ctx_last_device_ms) */
 #define BOLT_FLAG_FORCE_GLOBAL 0x4u  /* GROUP BY: skip the shared-memory tier (testing) */
 #define BOLT_FLAG_FORCE_SHMEM  0x8u  /* GROUP BY: shared-memory tier only; spill -> BOLT_ERR_SPILL */
+#define BOLT_FLAG_NO_TUNE      0x10u /* GROUP BY: ignore the context's autotuned choices */
 
 /* ------------------------------------------------------------------------ */
 /* Context: device, scratch arena, tuning cache, status word, last error.   */
@@ -192,6 +193,19 @@ typedef struct {
 bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc,
                          bolt_groupby_out* out, uint32_t flags, bolt_stream stream);
 
+/* Autotuner (replaces the reference's fixed dispatch thresholds,
+ * groupby_shmem_dispatch.rs:126-131, groupby_tier2_dispatch.rs:171-225):
+ * times the GROUP BY of `desc` on the device under candidate launch choices
+ * (thread-block size, shared-memory table size, warp pre-aggregation,
+ * hash-table load factor) and keeps the fastest for this query shape in the
+ * context; later calls of the same shape use it. `out` receives a valid
+ * result; best_ms (nullable) the winner's device time. */
+bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_desc* desc,
+                                  bolt_groupby_out* out, bolt_stream stream, double* best_ms);
+/* Saves / loads the context's tuning cache (text, one shape per line). */
+bolt_status bolt_ctx_tuning_save(const bolt_ctx* ctx, const char* path);
+bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path);
+
 /* ------------------------------------------------------------------------ */
 /* Hash join (INNER, single equi-key, I32/I64 keys, unique build keys).      */
 /* Replaces gpu_join::hash_join_indices_on_gpu{,_aos}                        */
@@ -289,6 +303,21 @@ bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* queries, int32_t n_que
 /* Scratch bytes bolt_groupby would use for a query (the serving admission
  * footprint). */
 uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64_t n_rows);
+
+/* A batch of queries captured once as a CUDA graph and replayed: the graph
+ * owns a private scratch arena and descriptor copies, so replays are
+ * independent of other calls. Every replay re-reads the queries' columns
+ * (so they may be updated in place between replays) and rewrites their
+ * outputs. Tables must be large enough for the data (no growth retries
+ * inside a graph): a query that would need one reports BOLT_ERR_SPILL in
+ * bolt_graph_sync_status. */
+typedef struct bolt_graph bolt_graph;
+bolt_status bolt_batch_graph_create(int device, bolt_query* queries, int32_t n_queries, bolt_graph** out);
+bolt_status bolt_graph_launch(bolt_graph* g, bolt_stream stream);
+/* Waits for the stream; fills per-query statuses and group counts (each
+ * array nullable, n_queries entries). Returns the first failing status. */
+bolt_status bolt_graph_sync_status(bolt_graph* g, bolt_stream stream, int32_t* statuses, uint64_t* n_groups);
+void        bolt_graph_destroy(bolt_graph* g);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: a request loop that keeps columns resident, admits queries by    */

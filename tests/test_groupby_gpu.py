@@ -225,3 +225,26 @@ def test_groupby_host_inputs_end_to_end(bolt, engine, oracle):
     orc = oracle.groupby({k: oracle.HostCol(v[0], v[2]) for k, v in cols.items()}, ["k"],
                          [("sum", "v"), ("count_star", None)])
     compare_groupby(res, orc, ["i32"], [("sum", "v"), ("count_star", None)], ["i64", None])
+
+
+def test_autotune_keeps_results_and_persists(bolt, engine, oracle, tmp_path):
+    cols = filtered_config(1_000_000, 100_000, seed=13)
+    dev, host = tables(bolt, oracle, cols)
+    base = engine.execute_groupby(dev, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)], groups_hint=100_000,
+                                  flags=bolt.FLAG_NO_TUNE)
+    pq = engine.prepare_groupby(dev, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], groups_hint=100_000)
+    best = engine.autotune_groupby(pq)
+    assert best > 0
+    tuned = engine.execute_groupby(dev, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)], groups_hint=100_000)
+    for x, y in zip(base.aggs + base.keys, tuned.aggs + tuned.keys):
+        xa = x.data.view(torch.int64) if x.data.dtype == torch.float64 else x.data
+        ya = y.data.view(torch.int64) if y.data.dtype == torch.float64 else y.data
+        assert torch.equal(xa, ya)
+    path = tmp_path / "tune.txt"
+    engine.save_tuning(path)
+    assert path.read_text().strip()
+    other = bolt.Engine(0, scratch_bytes=1 << 30)
+    try:
+        other.load_tuning(path)
+    finally:
+        other.close()
