@@ -28,7 +28,8 @@ from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLO
 
 __all__ = ["BoltError", "DeclineError", "SpillError", "TypeError_", "GpuCapacityError", "TimeoutError_",
            "CudaError", "PlanError", "Column", "Engine", "col", "GroupbyResult", "FLAG_ASYNC",
-           "FLAG_PROFILE", "FLAG_FORCE_GLOBAL", "FLAG_FORCE_SHMEM", "lib", "PreparedGroupby", "Server"]
+           "FLAG_PROFILE", "FLAG_FORCE_GLOBAL", "FLAG_FORCE_SHMEM", "FLAG_NO_TUNE", "lib", "PreparedGroupby",
+           "Server", "BatchGraph"]
 
 
 # ---------------------------------------------------------------------------
@@ -501,6 +502,54 @@ class PreparedGroupby:
             res.keys = [c.to("cpu") for c in res.keys]
             res.aggs = [c.to("cpu") for c in res.aggs]
         return res
+
+
+class BatchGraph:
+    """A batch of prepared GROUP BY queries captured once as a CUDA graph
+    (bolt_batch_graph_create) and replayed with one launch."""
+
+    def __init__(self, device: int, prepared: Sequence[PreparedGroupby]):
+        self._lib = lib()
+        self.prepared = list(prepared)
+        n = len(self.prepared)
+        self.qs = (_abi.Query * n)(*[pq.query() for pq in self.prepared])
+        h = C.c_void_p()
+        st = self._lib.bolt_batch_graph_create(device, self.qs, n, C.byref(h))
+        if st != _abi.OK:
+            raise _ERRORS.get(st, BoltError)(f"bolt_batch_graph_create failed: {_abi.STATUS_NAMES[st]}", st)
+        self._h = h
+        self.device = device
+
+    def launch(self, stream_handle: int | None = None):
+        s = stream_handle if stream_handle is not None else torch.cuda.current_stream(self.device).cuda_stream
+        st = self._lib.bolt_graph_launch(self._h, C.c_void_p(s))
+        if st != _abi.OK:
+            raise CudaError("bolt_graph_launch failed", st)
+
+    def results(self, stream_handle: int | None = None) -> list[GroupbyResult]:
+        s = stream_handle if stream_handle is not None else torch.cuda.current_stream(self.device).cuda_stream
+        n = len(self.prepared)
+        sts = (C.c_int32 * n)()
+        ng = (C.c_uint64 * n)()
+        st = self._lib.bolt_graph_sync_status(self._h, C.c_void_p(s), sts, ng)
+        if st != _abi.OK:
+            raise _ERRORS.get(st, BoltError)(f"batch graph replay: {_abi.STATUS_NAMES[st]}", st)
+        out = []
+        for i, pq in enumerate(self.prepared):
+            pq.out.n_groups = ng[i]
+            out.append(pq.result(False))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bolt_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

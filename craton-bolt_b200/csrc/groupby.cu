@@ -267,7 +267,7 @@ __device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored) {
 // `sk` / `sw` are the shared table's keys and state words (C slots, C may be 0).
 template <int U, int MAXS>
 __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull* sw, int C, uint64_t base,
-                                                uint32_t& inserts) {
+                                                uint32_t& inserts, uint32_t& absbits) {
     const int SW = p.slot_words - 1;
     const uint32_t lane = lane_id();
     const uint64_t n = p.n_rows;
@@ -341,6 +341,20 @@ __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull*
                 if (row && s < p.n_st)
                     contribution(p, p.st[s], raw[u][s], (vbits[u] >> s) & 1, (dfit[u] >> s) & 1,
                                  p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, c0[s], c1[s]);
+            }
+            // Bit length of the largest |v| fed to an int64 SUM: decides
+            // whether a row-order prefix of some group could leave the i64
+            // range (then the exact row-order check runs after the query).
+            if (row && p.i64_bits) {
+#pragma unroll
+                for (int s = 0; s < MAXS; ++s) {
+                    if (s < p.n_st && p.st[s].kind == K_SUM_I64 && ((vbits[u] >> s) & 1)) {
+                        const ll v = (ll)raw[u][s];
+                        const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
+                        const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
+                        absbits = b > absbits ? b : absbits;
+                    }
+                }
             }
             // Special groups: the NULL key and the key whose complement is 0.
             const bool special = row && (knull[u] || stored[u] == 0);
@@ -419,6 +433,13 @@ __device__ __forceinline__ bool gb_tile_epilogue(const GbParams& p, uint32_t& in
     return *s_stop != 0;
 }
 
+// Publishes the warp's largest |v| bit length for int64 SUMs (whole warp).
+__device__ __forceinline__ void gb_flush_absbits(const GbParams& p, uint32_t& absbits) {
+    const uint32_t m = __reduce_max_sync(0xffffffffu, absbits);
+    if (p.i64_bits && m && lane_id() == 0) atomicMax(p.i64_bits, m);
+    absbits = 0;
+}
+
 // Merges a CTA's shared table into the query's global table (whole CTA,
 // after a __syncthreads()).
 __device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk, const ull* sw, int C) {
@@ -455,11 +476,12 @@ __global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbP
     if (threadIdx.x == 0) { s_ins = 0; s_stop = 0; }
     __syncthreads();
     const uint64_t tile = (uint64_t)blockDim.x * U;
-    uint32_t inserts = 0;
+    uint32_t inserts = 0, absbits = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * tile; base < p.n_rows; base += (uint64_t)gridDim.x * tile) {
-        gb_process_tile<U, MAXS>(p, sk, sw, C, base, inserts);
+        gb_process_tile<U, MAXS>(p, sk, sw, C, base, inserts, absbits);
         if (gb_tile_epilogue(p, inserts, &s_ins, &s_stop)) return;
     }
+    gb_flush_absbits(p, absbits);
     __syncthreads();
     gb_flush_shared(p, sk, sw, C);
 }
@@ -708,6 +730,88 @@ bolt_status launch_agg(bolt_ctx* ctx, const GbPlan& pl, cudaStream_t s, size_t s
     return BOLT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Exact row-order check of int64 SUM (checked_group_sum, groupby.rs:1775):
+// only run when some group's partial sums could leave the i64 range.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t g_find(const GbParams& p, ull stored) {
+    const ull mask = (1ull << p.log2cap) - 1;
+    ull h = (stored * HASH_G) >> (64 - p.log2cap);
+    for (uint32_t i = 0; i < p.max_probe; ++i) {
+        const ull k = ld_volatile(p.gtab + h * (ull)p.slot_words);
+        if (k == stored) return (int64_t)h;
+        if (k == 0) return -1;
+        h = (h + 1) & mask;
+    }
+    return -1;
+}
+
+// Row -> group slot; rows that reach no group get ~0u.
+__global__ void __launch_bounds__(256) gb_row_slot_kernel(const __grid_constant__ GbParams p, uint32_t* slot_of_row) {
+    const ull cap = 1ull << p.log2cap;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n_rows;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = p.row_begin + i;
+        bool has = true;
+        for (int q = 0; q < p.n_pred; ++q) has = has && eval_pred(p.pred[q], r);
+        bool knull = false;
+        ull stored = 0;
+        if (p.jslots) {
+            if (!bit_valid(p.jkvalid, r)) has = false;
+            if (has) {
+                const ull k = p.jkdt == BOLT_I32 ? (ull)(ll)__ldg((const int32_t*)p.jkey + r) : (ull)__ldg((const ll*)p.jkey + r);
+                const ull w1 = join_lookup(p.jslots, p.jlog2cap, k);
+                if (w1 == ~0ull) has = false;
+                stored = ~(ull)(ll)(int32_t)(uint32_t)w1;
+            }
+        } else {
+            for (int k = 0; k < p.n_keys; ++k) knull = knull || !bit_valid(p.kvalid[k], r);
+            if (knull && p.n_keys > 1) has = false;
+            if (has && !knull) stored = ~pack_key(p, r);
+        }
+        uint32_t slot = 0xFFFFFFFFu;
+        if (has) {
+            if (knull) slot = (uint32_t)(cap + 1);
+            else if (stored == 0) slot = (uint32_t)cap;
+            else {
+                const int64_t g = g_find(p, stored);
+                if (g >= 0) slot = (uint32_t)g;
+            }
+        }
+        slot_of_row[i] = slot;
+    }
+}
+
+// One thread per run of equal slots in the stable (slot, row) order: replays
+// the group's int64 SUMs in row order and flags any prefix outside i64.
+__global__ void __launch_bounds__(256) gb_prefix_check_kernel(const __grid_constant__ GbParams p,
+                                                               const uint32_t* slot_of_row, const uint32_t* sorted) {
+    const uint64_t n = p.n_rows;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = slot_of_row[sorted[i]];
+        if (s == 0xFFFFFFFFu) continue;
+        if (i > 0 && slot_of_row[sorted[i - 1]] == s) continue;  // not the head of its run
+        for (int st = 0; st < p.n_st; ++st) {
+            const StateDesc& d = p.st[st];
+            if (d.kind != K_SUM_I64) continue;
+            ll acc = 0;
+            for (uint64_t j = i; j < n; ++j) {
+                const uint32_t row = sorted[j];
+                if (slot_of_row[row] != s) break;
+                const uint64_t r = p.row_begin + row;
+                if (!bit_valid(d.valid, r)) continue;
+                const ll v = __ldg((const ll*)d.col + r);
+                const ll nx = (ll)((ull)acc + (ull)v);
+                if ((v > 0 && nx < acc) || (v < 0 && nx > acc)) {
+                    atomicOr(p.status, ST_FLAG_OVERFLOW);
+                    break;
+                }
+                acc = nx;
+            }
+        }
+    }
+}
+
 // Persistent multi-query aggregation: work items are (query, tile of
 // blockDim.x * U rows) handed out in order from one counter. A CTA keeps one
 // query's shared table while its items stay on that query and merges it into
@@ -723,7 +827,7 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
     __shared__ int s_stop;
     int cur = -1;
     int C = 0;
-    uint32_t inserts = 0;
+    uint32_t inserts = 0, absbits = 0;
     if (threadIdx.x == 0) {
         s_ins = 0;
         s_stop = 0;
@@ -736,6 +840,7 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
         const int q = query_of(begins, nq, item);
         if (q != cur) {
             if (cur >= 0) {
+                gb_flush_absbits(p, absbits);
                 gb_flush_shared(p, smem, smem + C, C);
                 __syncthreads();
             }
@@ -753,10 +858,13 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
             continue;  // the query already flagged growth; the host re-runs it
         }
         const uint64_t base = (uint64_t)(item - begins[q]) * blockDim.x * U;
-        gb_process_tile<U, MAXS>(p, smem, smem + C, C, base, inserts);
+        gb_process_tile<U, MAXS>(p, smem, smem + C, C, base, inserts, absbits);
         gb_tile_epilogue(p, inserts, &s_ins, &s_stop);
     }
-    if (cur >= 0) gb_flush_shared(p, smem, smem + C, C);
+    if (cur >= 0) {
+        gb_flush_absbits(p, absbits);
+        gb_flush_shared(p, smem, smem + C, C);
+    }
 }
 
 }  // namespace
@@ -1029,6 +1137,9 @@ bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t
         f.n_groups = w + 2;
         f.status = p.status;
         pls[q]->words = w;
+        p.i64_bits = nullptr;
+        for (int s2 = 0; s2 < p.n_st; ++s2)
+            if (p.st[s2].kind == K_SUM_I64) p.i64_bits = (uint32_t*)(w + 4);
     }
 
     // Aggregation.
@@ -1177,6 +1288,37 @@ extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64
 
 namespace bolt {
 
+// The reference checks SUM(Int64) with a checked add in row order per group
+// (checked_group_sum, groupby.rs:1775-1798), so a prefix that leaves the
+// i64 range errors even when the final sum fits. When the largest |v| and
+// the row count allow such a prefix, replay every group's rows in row order
+// (stable radix sort of (slot, row), then one sequential fold per group).
+static bolt_status gb_exact_i64_check(bolt_ctx* ctx, GbPlan& pl, cudaStream_t s) {
+    const uint64_t n = pl.prm.n_rows;
+    if (n >= (1ull << 30))
+        return fail(ctx, BOLT_DECLINE, "GROUP BY: SUM(Int64) row-order overflow check needs < 2^30 rows");
+    uint32_t* slot_of_row = (uint32_t*)arena_alloc(ctx, n * 4 + 16);
+    uint32_t* sorted = (uint32_t*)arena_alloc(ctx, n * 4 + 16);
+    if (!slot_of_row || !sorted) return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the SUM check");
+    const unsigned g = grid_for(n, 256, ctx->num_sms * 8);
+    gb_row_slot_kernel<<<g, 256, 0, s>>>(pl.prm, slot_of_row);
+    SortSpec sp;
+    sp.src = SRC_U32;
+    SortSegment seg;
+    seg.keys = slot_of_row;
+    seg.n = n;
+    seg.payload_out = sorted;
+    sp.segs.push_back(seg);
+    bolt_status st = radix_sort(ctx, s, sp);
+    if (st != BOLT_OK) return st;
+    gb_prefix_check_kernel<<<g, 256, 0, s>>>(pl.prm, slot_of_row, sorted);
+    BOLT_CUDA(ctx, cudaGetLastError());
+    uint32_t f = 0;
+    st = read_status(ctx, s, 0, &f);
+    if (st != BOLT_OK) return st;
+    return flags_to_status(ctx, f, "GROUP BY");
+}
+
 // Runs one query (optionally with a join table as its key source) with the
 // retry policy: grow the table on GROW / SPILL, switch the f64 SUM to atomics
 // on RANGE, switch Decimal128 SUM to the wide state on DECRANGE.
@@ -1208,9 +1350,12 @@ static bolt_status gb_single(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_gro
         uint32_t f = 0;
         st = read_status(ctx, s, 0, &f);
         if (st != BOLT_OK) return st;
-        ull w[4] = {0, 0, 0, 0};
+        ull w[5] = {0, 0, 0, 0, 0};
         BOLT_CUDA(ctx, cudaMemcpy(w, pl.words, sizeof w, cudaMemcpyDeviceToHost));
         out->n_groups = w[2];
+        const uint32_t bits = (uint32_t)w[4];
+        if (f == 0 && pl.prm.i64_bits && bits + (uint32_t)ceil_log2_u64(pl.prm.n_rows + 1) >= 63)
+            return gb_exact_i64_check(ctx, pl, s);
         if (f & (ST_FLAG_GROW | ST_FLAG_SPILL)) {
             if (flags & BOLT_FLAG_FORCE_SHMEM)
                 return fail(ctx, BOLT_ERR_SPILL, "partition_reduce spill: shared-memory tier overflow");

@@ -56,7 +56,9 @@ struct AggOut {
     uint8_t* out_valid;
 };
 
-struct GbParams {
+// Both descriptors are copied into shared memory as 16-byte words, so their
+// sizes are multiples of 16 (alignas).
+struct alignas(16) GbParams {
     const void* kcol[2];
     const uint8_t* kvalid[2];
     int32_t kdtype[2];
@@ -77,6 +79,9 @@ struct GbParams {
     uint32_t* status;
     ull* occupancy;
     ull grow_limit;
+    // Largest bit length of |v| over int64 SUM inputs (nullptr when the
+    // query has no int64 SUM).
+    uint32_t* i64_bits;
     // Join source: when jslots is set the group key of a row is the payload
     // of the build slot its probe key matches (rows without a match are
     // skipped) instead of its packed key columns.
@@ -87,7 +92,7 @@ struct GbParams {
     const uint8_t* jkvalid;
 };
 
-struct GbFinal {
+struct alignas(16) GbFinal {
     ull* gtab;
     int32_t slot_words;
     int32_t log2cap;

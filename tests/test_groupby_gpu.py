@@ -167,6 +167,24 @@ def test_groupby_sum_i64_overflow(bolt, engine, oracle):
     assert "SUM(integer) overflow" in str(ei.value)
 
 
+@pytest.mark.parametrize("order,overflows", [((1, 1, -1, -1), True), ((1, -1, 1, -1), False)])
+def test_groupby_sum_i64_row_order_prefix_overflow(bolt, engine, oracle, order, overflows):
+    """checked_group_sum errors when a row-order prefix leaves i64 even if the
+    final sum fits; the GPU path reproduces that exactly."""
+    k = np.array([0, 1, 0, 1, 0, 1, 0, 1], np.int32)
+    v = np.array([s * 2**62 for s in order for _ in range(2)], np.int64)
+    dev, host = tables(bolt, oracle, {"k": (k, None, "i32", 0), "v": (v, None, "i64", 0)})
+    if overflows:
+        with pytest.raises(bolt.TypeError_):
+            engine.execute_groupby(dev, ["k"], [("sum", "v")])
+        with pytest.raises(oracle.OracleError):
+            oracle.groupby(host, ["k"], [("sum", "v")])
+    else:
+        res = engine.execute_groupby(dev, ["k"], [("sum", "v")])
+        assert res.aggs[0].numpy().tolist() == [0, 0]
+        assert oracle.groupby(host, ["k"], [("sum", "v")])["vals"][0].tolist() == [0, 0]
+
+
 def test_groupby_empty_input_and_all_filtered(bolt, engine, oracle):
     k = np.zeros(0, np.int32)
     v = np.zeros(0, np.int64)
