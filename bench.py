@@ -46,8 +46,20 @@ from pathlib import Path
 
 import numpy as np
 
+import faulthandler
+
+faulthandler.enable()  # a native crash prints every thread's Python stack to stderr
+
 REPO = Path(__file__).resolve().parent
-METRIC = "rows/s & HBM GB/s (of ~8 TB/s) per operator; batched q/s + p99 vs per-query"
+
+
+def progress(msg: str):
+    """Progress marker on stderr (stdout carries only the JSON line)."""
+    sys.stderr.write(f"[bench {time.strftime('%H:%M:%S')}] {msg}\n")
+    sys.stderr.flush()
+
+
+METRIC ="rows/s & HBM GB/s (of ~8 TB/s) per operator; batched q/s + p99 vs per-query"
 
 
 def load_package():
@@ -219,7 +231,7 @@ class Ctx:
     def timed(self, step, steps: int, warmup: int):
         """Runs warmup + K async steps; returns (device ms, launches, kernel ms list, clocks)."""
         torch = self.torch
-        sampler = ClockSampler(self.local)
+        sampler = ClockSampler(self.local) if not self.args.no_clocks else ClockSampler(-1)
         sampler.start()
         for _ in range(warmup):
             step()
@@ -326,15 +338,19 @@ def cpu_rows_per_s_groupby(table_np: dict, dts: dict, group_by, aggs, where, n_s
 def w_groupby_filtered(c: Ctx):
     a = c.args
     torch = c.torch
+    progress(f"generating {a.rows} rows")
     data = gen_filtered(a.rows, c.dev)
+    progress("pinning and uploading")
     host = {k: torch.from_numpy(v).pin_memory() for k, v in data.items()}
     dev = {k: c.bolt.Column(host[k].to(c.dev), FILTERED_DT[k]) for k in data}
     torch.cuda.synchronize()
+    progress("prepared; timing")
     pq = c.eng.prepare_groupby(dev, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], groups_hint=a.groups_hint,
                                out_cap=max(2 * a.groups_hint, 1 << 20))
     call = PreparedCall(c, pq)
     ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
     n_groups = int(call.ng.item())
+    progress(f"timed: {ms / a.steps:.3f} ms/step, {n_groups} groups")
     alg = a.rows * FILTERED_BYTES
     line = base_line(c, ms, a.rows, alg, kms, "gb_agg_kernel", "groupby_filtered",
                      {"workload": "filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) ranks, "
@@ -350,11 +366,13 @@ def w_groupby_filtered(c: Ctx):
             res["r"] = c.eng.execute_groupby(hcols, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
                                              groups_hint=a.groups_hint)
 
+        progress("end-to-end")
         e_ms = c.time_e2e(e2e, a.e2e_steps)
         line["e2e"] = {"value": c.world * a.rows / (e_ms * 1e-3), "unit": "rows/s", "h2d_bytes_per_step": alg,
                        "d2h_bytes_per_step": res["r"].n_groups * (4 + 4 + 8 * 5), "ms_per_step": e_ms,
                        "path": "Engine.execute_groupby on pinned host columns (H2D + GROUP BY + D2H)"}
     if c.world == 1 and not a.no_cpu:
+        progress("CPU baseline")
         ns = min(a.cpu_rows, a.rows)
         rps = cpu_rows_per_s_groupby(data, FILTERED_DT, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], ns)
         line["cpu_baseline"] = {"value": rps, "unit": "rows/s", "cores": 1, "kind": "port",
@@ -715,6 +733,7 @@ def main():
     ap.add_argument("--cpu-rows", type=int, default=10_000_000)
     ap.add_argument("--reference-rows", type=int, default=2_000_000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -723,7 +742,9 @@ def main():
         if rank == 0:
             run_reference(args)
         return
+    progress(f"workload {args.workload}")
     c = Ctx(args)
+    progress("context ready")
     line = WORKLOADS[args.workload](c)
     if c.rank == 0:
         print(json.dumps(line), flush=True)

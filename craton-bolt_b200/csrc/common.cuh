@@ -24,6 +24,23 @@ enum : uint32_t {
     ST_FLAG_DECOVERFLOW = 1u << 8,  // SUM(Decimal128) outside the i128 range
 };
 
+// Bytes per row of a column dtype (0 for an unknown dtype).
+__host__ __device__ __forceinline__ int dtype_width(int dt) {
+    switch (dt) {
+    case BOLT_I32: case BOLT_F32: case BOLT_U32: return 4;
+    case BOLT_I64: case BOLT_F64: return 8;
+    case BOLT_DEC128: return 16;
+    }
+    return 0;
+}
+
+// A column's data pointer must be aligned to its element width (kernels use
+// native-width and 16-byte vector accesses); checked on the host.
+inline bool col_aligned(const void* p, int dt) {
+    const int w = dtype_width(dt);
+    return w != 0 && (reinterpret_cast<uintptr_t>(p) % (uintptr_t)w) == 0;
+}
+
 // ---- bit-level helpers ----------------------------------------------------
 __host__ __device__ __forceinline__ int ceil_log2_u64(uint64_t x) {
     int r = 0;

@@ -219,6 +219,8 @@ bolt_status compact_common(bolt_ctx* ctx, const bolt_col_view* cols, int32_t n_c
         const int wd = width_of(cols[c].dtype);
         if (!wd || !out || out[c].dtype != cols[c].dtype)
             return fail(ctx, BOLT_ERR_INVALID, "compaction: column %d dtype mismatch", c);
+        if (!col_aligned(cols[c].data, cols[c].dtype) || !col_aligned(out[c].data, cols[c].dtype))
+            return fail(ctx, BOLT_ERR_INVALID, "compaction: column %d is not aligned to its element width", c);
         sp.col[c] = CompactCol{cols[c].data, cols[c].validity, out[c].data, cols[c].validity ? out[c].validity : nullptr, wd};
         sp.out_cap = sp.out_cap < out[c].cap ? sp.out_cap : out[c].cap;
     }

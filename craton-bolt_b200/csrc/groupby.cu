@@ -911,6 +911,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         const bolt_col_view* c = col(d->key_cols[k]);
         if (!c) return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: key column %d out of range", d->key_cols[k]);
         if (c->len < row_end) return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: key column shorter than the rows");
+        if (!col_aligned(c->data, c->dtype))
+            return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: key column %d is not aligned to its element width", k);
         const int dt = c->dtype;
         const bool ok = d->n_keys == 1 ? (dt == BOLT_I32 || dt == BOLT_I64 || dt == BOLT_F32 || dt == BOLT_F64)
                                        : (dt == BOLT_I32 || dt == BOLT_F32);
@@ -921,6 +923,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         f.kdtype[k] = dt;
         if (!out->keys || out->keys[k].dtype != dt)
             return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: output key column %d dtype mismatch", k);
+        if (!col_aligned(out->keys[k].data, dt))
+            return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: output key column %d is not aligned", k);
         f.out_key[k] = out->keys[k].data;
         f.out_key_valid[k] = out->keys[k].validity;
     }
@@ -930,6 +934,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         if (!c) return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: WHERE column out of range");
         if (c->dtype == BOLT_DEC128 || c->dtype == BOLT_U32)
             return fail(ctx, BOLT_DECLINE, "GROUP BY: WHERE on dtype %d", c->dtype);
+        if (!col_aligned(c->data, c->dtype))
+            return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: WHERE column %d is not aligned to its element width", q);
         p.pred[q] = PredDesc{c->data, c->validity, c->dtype, d->preds[q].cmp, d->preds[q].lit_i, d->preds[q].lit_f};
     }
     p.n_pred = d->n_preds;
@@ -966,6 +972,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         if (sp.op != BOLT_AGG_COUNT_STAR && !c)
             return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: aggregate %d input column out of range", a);
         if (c && c->len < row_end) return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: value column shorter than the rows");
+        if (c && !col_aligned(c->data, c->dtype))
+            return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: aggregate %d input is not aligned to its element width", a);
         const int dt = c ? c->dtype : BOLT_I64;
         g.in_dtype = dt;
         g.nullable = c && c->validity ? 1 : 0;
@@ -1015,6 +1023,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         if (missing) return fail(ctx, BOLT_DECLINE, "GROUP BY: more than %d aggregate states", GB_MAX_STATES);
         if (!out->aggs || out->aggs[a].dtype != g.out_dtype)
             return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: output column %d must have dtype %d", a, g.out_dtype);
+        if (!col_aligned(out->aggs[a].data, g.out_dtype))
+            return fail(ctx, BOLT_ERR_INVALID, "GROUP BY: output column %d is not aligned to its element width", a);
         g.out = out->aggs[a].data;
         g.out_valid = out->aggs[a].validity;
     }
@@ -1398,6 +1408,8 @@ extern "C" bolt_status bolt_join_groupby(bolt_ctx* ctx, const bolt_join_table* t
     if (probe_key->dtype != BOLT_I32 && probe_key->dtype != BOLT_I64)
         return fail(ctx, BOLT_DECLINE, "join GROUP BY: probe key dtype %d", probe_key->dtype);
     if (value->len != probe_key->len) return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: column lengths differ");
+    if (!col_aligned(probe_key->data, probe_key->dtype))
+        return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: probe key is not aligned to its element width");
     // Column 0 stands for the group key (its data is never read in join mode).
     bolt_col_view cols[2] = {*probe_key, *value};
     cols[0].dtype = BOLT_I32;

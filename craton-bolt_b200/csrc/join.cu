@@ -193,6 +193,8 @@ extern "C" bolt_status bolt_hash_join_build(bolt_ctx* ctx, const bolt_col_view* 
         return fail(ctx, BOLT_DECLINE, "hash join build: key dtype %d (Int32/Int64 supported)", build_key->dtype);
     if (payload && (payload->dtype != BOLT_I32 || payload->len != build_key->len))
         return fail(ctx, BOLT_ERR_INVALID, "hash join build: payload must be an Int32 column of the build length");
+    if (!col_aligned(build_key->data, build_key->dtype) || (payload && !col_aligned(payload->data, BOLT_I32)))
+        return fail(ctx, BOLT_ERR_INVALID, "hash join build: columns must be aligned to their element width");
     const uint64_t n = build_key->len;
     if (n >= 0xFFFFFFFFull) return fail(ctx, BOLT_DECLINE, "hash join build: %llu rows exceed u32 row ids", (ull)n);
     cudaStream_t s = (cudaStream_t)stream;
@@ -254,6 +256,9 @@ extern "C" bolt_status bolt_hash_join_probe(bolt_ctx* ctx, const bolt_join_table
     if (probe_idx->dtype != BOLT_U32 || build_idx->dtype != BOLT_U32)
         return fail(ctx, BOLT_ERR_INVALID, "hash join probe: index outputs must be U32");
     if (probe_key->len >= 0xFFFFFFFFull) return fail(ctx, BOLT_DECLINE, "hash join probe: too many probe rows");
+    if (!col_aligned(probe_key->data, probe_key->dtype) || !col_aligned(probe_idx->data, BOLT_U32) ||
+        !col_aligned(build_idx->data, BOLT_U32))
+        return fail(ctx, BOLT_ERR_INVALID, "hash join probe: columns must be aligned to their element width");
     cudaStream_t s = (cudaStream_t)stream;
     bolt_status st = call_begin(ctx, flags, s);
     if (st != BOLT_OK) return st;

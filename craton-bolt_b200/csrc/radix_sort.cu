@@ -480,6 +480,8 @@ extern "C" bolt_status bolt_radix_sort_perm_multi(bolt_ctx* ctx, const bolt_col_
     for (int k = 0; k < n_keys; ++k) {
         if (keys[k].len != n) return fail(ctx, BOLT_ERR_INVALID, "ORDER BY: key lengths differ");
         if (sort_src_of(keys[k].dtype) < 0) return fail(ctx, BOLT_DECLINE, "ORDER BY: key dtype %d", keys[k].dtype);
+        if (!col_aligned(keys[k].data, keys[k].dtype))
+            return fail(ctx, BOLT_ERR_INVALID, "ORDER BY: key %d is not aligned to its element width", k);
     }
     if (perm->dtype != BOLT_U32 || perm->cap < n) return fail(ctx, BOLT_ERR_CAPACITY, "ORDER BY: permutation output too small");
     if (n >= (1ull << 30)) return fail(ctx, BOLT_DECLINE, "ORDER BY: %llu rows exceed 2^30", (ull)n);
