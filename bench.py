@@ -59,7 +59,7 @@ def progress(msg: str):
     sys.stderr.flush()
 
 
-METRIC ="rows/s & HBM GB/s (of ~8 TB/s) per operator; batched q/s + p99 vs per-query"
+METRIC = "rows/s & HBM GB/s (of ~8 TB/s) per operator; batched q/s + p99 vs per-query"
 
 
 def load_package():
@@ -109,34 +109,39 @@ def profiled_traffic(workload: str):
 # Clock sampling (NVML) during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    def __init__(self, device_index: int, period_s: float = 0.005):
+    """Samples SM clock and throttle reasons with `nvidia-smi -lms` in a child
+    process (a separate process cannot take the benchmark down with it)."""
+
+    FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int, period_ms: int = 50):
         self.samples = []
-        self.period = period_s
-        self._stop = threading.Event()
         self.ok = False
+        self.proc = None
         try:
-            import pynvml
+            import subprocess
+
             import torch
 
-            pynvml.nvmlInit()
+            if device_index < 0:
+                raise RuntimeError("clock sampling disabled")
             bus = torch.cuda.get_device_properties(device_index).pci_bus_id
-            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode() if isinstance(bus, str) else bus)
-            self.nv = pynvml
-            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.bus_tail = bus.upper()[-7:]  # "1B:00.0"
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", str(period_ms)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.ok = True
         except Exception as e:  # noqa: BLE001
             self.err = str(e)
 
     def _run(self):
-        nv = self.nv
-        while not self._stop.is_set():
-            try:
-                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
-                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-                self.samples.append((time.perf_counter(), mhz, rs))
-            except Exception:  # noqa: BLE001
-                pass
-            time.sleep(self.period)
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or not parts[0].upper().endswith(self.bus_tail):
+                continue
+            self.samples.append((time.perf_counter(), parts))
 
     def start(self):
         if self.ok:
@@ -145,8 +150,12 @@ class ClockSampler:
 
     def stop(self):
         if self.ok:
-            self._stop.set()
-            self.t.join()
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+            self.t.join(timeout=5)
 
     def summary(self, t0: float, t1: float):
         if not self.ok:
@@ -156,23 +165,21 @@ class ClockSampler:
         if len(inside) < 3:
             inside = self.samples
             note = "timed region shorter than the sampling period: warm-up and timed samples"
-        nv = self.nv
-        names = {
-            "applications_clocks_setting": getattr(nv, "nvmlClocksEventReasonApplicationsClocksSetting", 0x2),
-            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
-            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
-            "sync_boost": getattr(nv, "nvmlClocksEventReasonSyncBoost", 0x10),
-            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
-            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
-            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
-        }
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        mhz = [num(p[1]) for _, p in inside if num(p[1]) is not None]
+        mx = [num(p[2]) for _, p in inside if num(p[2]) is not None]
         reasons = set()
-        for _, _, rs in inside:
-            for k, bit in names.items():
-                if rs & bit:
-                    reasons.add(k)
-        mhz = [s[1] for s in inside]
-        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": self.max_mhz,
+        for _, p in inside:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(inside), "note": note}
 
 
@@ -347,6 +354,12 @@ def w_groupby_filtered(c: Ctx):
     progress("prepared; timing")
     pq = c.eng.prepare_groupby(dev, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], groups_hint=a.groups_hint,
                                out_cap=max(2 * a.groups_hint, 1 << 20))
+    tuned = None
+    if not a.no_tune:
+        progress("autotuning")
+        best = c.eng.autotune_groupby(pq)
+        tuned = {"best_ms": best}
+        progress(f"autotuned: {best:.3f} ms")
     call = PreparedCall(c, pq)
     ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
     n_groups = int(call.ng.item())
@@ -356,6 +369,7 @@ def w_groupby_filtered(c: Ctx):
                      {"workload": "filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) ranks, "
                                   "WHERE f < 50, SUM/AVG(vd f64), COUNT(*), MIN/MAX(vi i64)",
                       "rows": a.rows, "groups": n_groups, "groups_hint": a.groups_hint,
+                      "autotuned": tuned,
                       "l2": "inputs (2.8 GB) larger than L2 (126 MB); no flush needed"},
                      launches, clocks, "int64/f64")
     if a.e2e_steps > 0:
@@ -734,6 +748,7 @@ def main():
     ap.add_argument("--reference-rows", type=int, default=2_000_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the GROUP BY autotuner")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

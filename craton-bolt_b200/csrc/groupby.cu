@@ -32,6 +32,7 @@
 #include "radix_sort.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 namespace bolt {
@@ -197,6 +198,80 @@ __device__ __forceinline__ void merge_words(ull* w, int kind, ull c0, ull c1) {
     }
     case K_SUM_FATOM: atomicAdd(reinterpret_cast<double*>(w), __longlong_as_double((ll)c0)); break;
     default: atomicMax(w, c0); break;
+    }
+}
+
+// ---- shared-memory merge built from native 32-bit atomics -----------------
+// 64-bit add / max on shared memory have no single native instruction; a
+// compiler-generated compare-and-swap loop serialises badly when many warps
+// hit one hot group. These variants use native 32-bit atomicAdd on the
+// words' halves with the carry of each limb computed from that atomic's own
+// old value (so concurrent adds still sum exactly, modulo the word width),
+// and MIN/MAX read first and CAS only when the new value would win.
+__device__ __forceinline__ void s32_add64(ull* w, ull x) {
+    uint32_t* p = reinterpret_cast<uint32_t*>(w);
+    const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32);
+    uint32_t carry = 0;
+    if (xl) {
+        const uint32_t old = atomicAdd(p, xl);
+        carry = (uint32_t)(((ull)old + xl) >> 32);
+    }
+    const uint32_t h = xh + carry;  // modulo 2^32, as the word is
+    if (h) atomicAdd(p + 1, h);
+}
+
+// 128-bit add of (x0 low, x1 high) into w[0..1], limb by limb.
+__device__ __forceinline__ void s32_add128(ull* w, ull x0, ull x1) {
+    uint32_t* p = reinterpret_cast<uint32_t*>(w);
+    const uint32_t x[4] = {(uint32_t)x0, (uint32_t)(x0 >> 32), (uint32_t)x1, (uint32_t)(x1 >> 32)};
+    uint32_t carry = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const ull add = (ull)x[i] + carry;
+        if (add == 0) {
+            carry = 0;
+            continue;
+        }
+        const uint32_t a32 = (uint32_t)add;
+        if (i == 3) {
+            if (a32) atomicAdd(p + 3, a32);
+            break;
+        }
+        if (a32 == 0) {  // add == 2^32: this limb unchanged, carry one out
+            carry = 1;
+            continue;
+        }
+        const uint32_t old = atomicAdd(p + i, a32);
+        carry = (uint32_t)(((ull)old + a32) >> 32);
+    }
+}
+
+__device__ __forceinline__ void s32_max64(ull* w, ull x) {
+    ull cur = *reinterpret_cast<volatile ull*>(w);
+    while (x > cur) {
+        const ull old = atomicCAS(w, cur, x);
+        if (old == cur) break;
+        cur = old;
+    }
+}
+
+__device__ __forceinline__ void merge_words_s32(ull* w, int kind, ull c0, ull c1) {
+    if ((c0 | c1) == 0) return;
+    switch (kind) {
+    case K_COUNT:
+    case K_SUM_I32: s32_add64(w, c0); break;
+    case K_SUM_I64:
+    case K_SUM_D64:
+        if (c0) s32_add64(w, c0);
+        if (c1) s32_add64(w + 1, c1);
+        break;
+    case K_SUM_FX: s32_add128(w, c0, c1); break;
+    case K_SUM_D128:
+        s32_add128(w, c0, c1 & 0xFFFFFFFFull);
+        if ((ll)c1 >> 32) s32_add64(w + 2, (ull)((ll)c1 >> 32));
+        break;
+    case K_SUM_FATOM: atomicAdd(reinterpret_cast<double*>(w), __longlong_as_double((ll)c0)); break;
+    default: s32_max64(w, c0); break;
     }
 }
 
@@ -397,9 +472,15 @@ __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull*
             if (C) sl = s_find_insert(sk, p.smem_log2, stored[u]);
             if (sl >= 0) {
                 ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
+                if (p.smem32) {
 #pragma unroll
-                for (int s = 0; s < MAXS; ++s)
-                    if (s < p.n_st) merge_words(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
+                    for (int s = 0; s < MAXS; ++s)
+                        if (s < p.n_st) merge_words_s32(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
+                } else {
+#pragma unroll
+                    for (int s = 0; s < MAXS; ++s)
+                        if (s < p.n_st) merge_words(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
+                }
             } else {
                 int64_t g = g_find_insert(p, stored[u], inserts);
                 if (g >= 0) {
@@ -1042,7 +1123,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
 
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
     pl->shape = gb_shape_key(p, n, d->groups_hint);
-    bolt_ctx::GbTune tn{512, 0, 0, 1, 0.0};
+    bolt_ctx::GbTune tn{512, 0, 1, 1, 1, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
@@ -1066,6 +1147,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     p.fx_e = 126 - 32 - ceil_log2_u64(n + 1);
     f.fx_e = p.fx_e;
     p.warp_agg = tn.warp_agg;
+    p.smem32 = tn.smem32;
     for (int s = 0; s < n_st; ++s)
         if (p.st[s].kind == K_SUM_D128) p.warp_agg = 0;  // D128 partials do not combine in registers
 
@@ -1508,10 +1590,15 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
     if (st != BOLT_OK) return st;
     std::vector<bolt_ctx::GbTune> cands;
     for (int block : {256, 512})
-        for (int smem_shift : {0, 1, 2, 8})
+        for (int smem_shift : {0, 1, 8})
             for (int warp_agg : {0, 1})
-                for (int load_shift : {1, 2}) cands.push_back({block, smem_shift, warp_agg, load_shift, 0.0});
-    bolt_ctx::GbTune best{512, 0, 0, 1, 1e30};
+                for (int load_shift : {1, 2})
+                    for (int smem32 : {0, 1}) {
+                        if (smem_shift == 8 && smem32) continue;  // no shared tier: smem32 is moot
+                        cands.push_back({block, smem_shift, warp_agg, load_shift, smem32, 0.0});
+                    }
+    bolt_ctx::GbTune best{512, 0, 1, 1, 1, 1e30};
+    const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
     for (auto& c : cands) {
         double tot = 0.0;
@@ -1539,6 +1626,9 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             BOLT_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
             if (rep > 0) tot += ms;  // first repetition warms up
         }
+        if (verbose)
+            std::fprintf(stderr, "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem32=%d -> %s%.4f ms\n",
+                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem32, ok ? "" : "(flagged) ", tot / 2);
         if (ok && tot / 2 < best.ms) {
             best = c;
             best.ms = tot / 2;
@@ -1555,8 +1645,8 @@ extern "C" bolt_status bolt_ctx_tuning_save(const bolt_ctx* ctx, const char* pat
     FILE* fp = std::fopen(path, "w");
     if (!fp) return BOLT_ERR_INVALID;
     for (const auto& kv : ctx->tune)
-        std::fprintf(fp, "%llx %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
-                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.ms);
+        std::fprintf(fp, "%llx %d %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
+                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.smem32, kv.second.ms);
     std::fclose(fp);
     return BOLT_OK;
 }
@@ -1567,10 +1657,11 @@ extern "C" bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path) {
     if (!fp) return fail(ctx, BOLT_ERR_INVALID, "tuning file %s not readable", path);
     unsigned long long key;
     bolt_ctx::GbTune t{};
-    while (std::fscanf(fp, "%llx %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift, &t.ms) == 6) {
+    while (std::fscanf(fp, "%llx %d %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift,
+                       &t.smem32, &t.ms) == 7) {
         const bool valid = (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
                            t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 1 &&
-                           t.load_shift <= 3;
+                           t.load_shift <= 3 && (t.smem32 == 0 || t.smem32 == 1);
         if (valid) ctx->tune[(uint64_t)key] = t;
     }
     std::fclose(fp);
