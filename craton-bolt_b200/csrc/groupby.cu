@@ -113,12 +113,12 @@ __device__ __forceinline__ ull order_key(ull raw, int dt) {
 }
 
 // Contribution (c0, c1) of one row to one state; zero words are the identity.
-__device__ __forceinline__ void contribution(const GbParams& p, const StateDesc& s, ull raw, bool valid,
+__device__ __forceinline__ void contribution(const GbParams& p, const StateDesc& s, int kind, ull raw, bool valid,
                                              bool dec_fits, uint64_t r, ull& c0, ull& c1) {
     c0 = 0;
     c1 = 0;
     if (!valid) return;
-    switch (s.kind) {
+    switch (kind) {
     case K_COUNT: c0 = 1; break;
     case K_SUM_I32: c0 = raw; break;
     case K_SUM_D64:
@@ -337,181 +337,226 @@ __device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored) {
 // ---------------------------------------------------------------------------
 // Aggregation kernel
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Aggregate-state layouts the row loop is compiled for. A runtime switch over
+// state kinds inside the unrolled row loop costs ~1,500 instructions per row
+// and thrashes the instruction cache; the common layouts (states sorted by
+// kind, see gb_plan) get a loop with the kinds known at compile time, and
+// everything else runs the generic loop.
+// ---------------------------------------------------------------------------
+struct SpecGeneric {
+    static constexpr bool generic = true;
+    static constexpr int n = 0;
+    __host__ __device__ static constexpr int kind(int) { return 0; }
+};
+template <int N, int K0, int K1 = 0, int K2 = 0, int K3 = 0>
+struct SpecK {
+    static constexpr bool generic = false;
+    static constexpr int n = N;
+    __host__ __device__ static constexpr int kind(int s) { return s == 0 ? K0 : s == 1 ? K1 : s == 2 ? K2 : K3; }
+};
+// Spec ids shared with the planner (gb_spec_of).
+using Spec1 = SpecK<4, K_COUNT, K_SUM_FX, K_MAX_ORD, K_MIN_ORD>;   // COUNT, SUM/AVG f64, MAX, MIN
+using Spec2 = SpecK<4, K_COUNT, K_SUM_I64, K_MAX_ORD, K_MIN_ORD>;  // COUNT, SUM i64, MAX, MIN
+using Spec3 = SpecK<2, K_COUNT, K_SUM_D64>;                        // COUNT, SUM Decimal128
+using Spec4 = SpecK<2, K_COUNT, K_SUM_I64>;                        // COUNT, SUM i64
+using Spec5 = SpecK<2, K_COUNT, K_SUM_FX>;                         // COUNT, SUM f64
+using Spec6 = SpecK<1, K_COUNT>;                                   // COUNT
+using Spec7 = SpecK<2, K_COUNT, K_SUM_I32>;                        // COUNT, SUM i32
+
+template <class SP>
+__device__ __forceinline__ int skind(const GbParams& p, int s) {
+    if constexpr (SP::generic) return p.st[s].kind;
+    else return SP::kind(s);
+}
+template <class SP>
+__device__ __forceinline__ int snum(const GbParams& p) {
+    if constexpr (SP::generic) return p.n_st;
+    else return SP::n;
+}
+
 // One tile of blockDim.x * U rows starting at row `base` of the query:
 // load, filter, key, pre-aggregate and fold into the shared or global table.
 // `sk` / `sw` are the shared table's keys and state words (C slots, C may be 0).
-template <int U, int MAXS>
+template <int U, int MAXS, class SP>
 __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull* sw, int C, uint64_t base,
                                                 uint32_t& inserts, uint32_t& absbits) {
     const int SW = p.slot_words - 1;
     const uint32_t lane = lane_id();
     const uint64_t n = p.n_rows;
-    {
-        bool has[U];
-        bool knull[U];
-        ull stored[U];
-        ull raw[U][MAXS];
-        uint32_t vbits[U];
-        uint32_t dfit[U];
-        // Issue every column load of the tile before any predicate resolves:
-        // all sectors are read anyway at the selectivities of interest, and
-        // independent loads keep more bytes in flight per SM.
+    const int NS = snum<SP>(p);
+    bool has[U];
+    bool knull[U];
+    ull stored[U];
+    ull raw[U][MAXS];
+    uint32_t vbits[U];
+    uint32_t dfit[U];
+    // Issue every column load of the tile before any predicate resolves:
+    // all sectors are read anyway at the selectivities of interest, and
+    // independent loads keep more bytes in flight per SM.
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const uint64_t i = base + (uint64_t)u * blockDim.x + threadIdx.x;
+        const uint64_t r = p.row_begin + i;
+        has[u] = i < n;
+        knull[u] = false;
+        stored[u] = 0;
+        vbits[u] = 0;
+        dfit[u] = 0;
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) raw[u][s] = 0;
+        if (!has[u]) continue;
+        if (p.jslots) {
+            if (bit_valid(p.jkvalid, r))
+                stored[u] = p.jkdt == BOLT_I32 ? (ull)(ll)ld_stream((const int32_t*)p.jkey + r)
+                                               : (ull)ld_stream((const ll*)p.jkey + r);
+            else
+                has[u] = false;
+        } else {
+            stored[u] = ~pack_key(p, r);
+        }
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+            if (s < NS && p.st[s].col) {
+                bool fits = true;
+                raw[u][s] = load_raw(p.st[s], r, fits);
+                if (bit_valid(p.st[s].valid, r)) vbits[u] |= 1u << s;
+                if (fits) dfit[u] |= 1u << s;
+            } else if (s < NS) {
+                vbits[u] |= 1u << s;  // COUNT(*)
+                dfit[u] |= 1u << s;
+            }
+        }
+        for (int q = 0; q < p.n_pred; ++q) has[u] = has[u] && eval_pred(p.pred[q], r);
+        if (!p.jslots)
+            for (int k = 0; k < p.n_keys; ++k) knull[u] = knull[u] || !bit_valid(p.kvalid[k], r);
+        if (knull[u] && p.n_keys > 1) has[u] = false;  // multi-key: NULL-key rows are dropped
+    }
+    if (p.jslots) {
+        // Join source: stored[u] holds the probe key; its group key is the
+        // matched build row's payload. All U lookups are issued together.
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint64_t i = base + (uint64_t)u * blockDim.x + threadIdx.x;
-            const uint64_t r = p.row_begin + i;
-            has[u] = i < n;
-            knull[u] = false;
-            stored[u] = 0;
-            vbits[u] = 0;
-            dfit[u] = 0;
-#pragma unroll
-            for (int s = 0; s < MAXS; ++s) raw[u][s] = 0;
             if (!has[u]) continue;
-            if (p.jslots) {
-                if (bit_valid(p.jkvalid, r))
-                    stored[u] = p.jkdt == BOLT_I32 ? (ull)(ll)ld_stream((const int32_t*)p.jkey + r)
-                                                   : (ull)ld_stream((const ll*)p.jkey + r);
-                else
-                    has[u] = false;
-            } else {
-                stored[u] = ~pack_key(p, r);
-            }
+            const ull w1 = join_lookup(p.jslots, p.jlog2cap, stored[u]);
+            if (w1 == ~0ull) has[u] = false;
+            stored[u] = ~(ull)(ll)(int32_t)(uint32_t)w1;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        bool row = has[u];
+        ull c0[MAXS], c1[MAXS];
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+            c0[s] = 0;
+            c1[s] = 0;
+            if (row && s < NS)
+                contribution(p, p.st[s], skind<SP>(p, s), raw[u][s], (vbits[u] >> s) & 1, (dfit[u] >> s) & 1,
+                             p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, c0[s], c1[s]);
+        }
+        // Bit length of the largest |v| fed to an int64 SUM: decides whether
+        // a row-order prefix of some group could leave the i64 range (then
+        // the exact row-order check runs after the query).
+        if (row && p.i64_bits) {
 #pragma unroll
             for (int s = 0; s < MAXS; ++s) {
-                if (s < p.n_st && p.st[s].col) {
-                    bool fits = true;
-                    raw[u][s] = load_raw(p.st[s], r, fits);
-                    if (bit_valid(p.st[s].valid, r)) vbits[u] |= 1u << s;
-                    if (fits) dfit[u] |= 1u << s;
-                } else if (s < p.n_st) {
-                    vbits[u] |= 1u << s;  // COUNT(*)
-                    dfit[u] |= 1u << s;
+                if (s < NS && skind<SP>(p, s) == K_SUM_I64 && ((vbits[u] >> s) & 1)) {
+                    const ll v = (ll)raw[u][s];
+                    const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
+                    const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
+                    absbits = b > absbits ? b : absbits;
                 }
             }
-            for (int q = 0; q < p.n_pred; ++q) has[u] = has[u] && eval_pred(p.pred[q], r);
-            if (!p.jslots)
-                for (int k = 0; k < p.n_keys; ++k) knull[u] = knull[u] || !bit_valid(p.kvalid[k], r);
-            if (knull[u] && p.n_keys > 1) has[u] = false;  // multi-key: NULL-key rows are dropped
         }
-        if (p.jslots) {
-            // Join source: stored[u] holds the probe key; its group key is the
-            // matched build row's payload. All U lookups are issued together.
+        // Special groups: the NULL key and the key whose complement is 0.
+        const bool special = row && (knull[u] || stored[u] == 0);
+        if (special) {
+            const ull slot = (1ull << p.log2cap) + (knull[u] ? 1 : 0);
+            ull* w = p.gtab + slot * (ull)p.slot_words;
+            if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (!has[u]) continue;
-                const ull w1 = join_lookup(p.jslots, p.jlog2cap, stored[u]);
-                if (w1 == ~0ull) has[u] = false;
-                stored[u] = ~(ull)(ll)(int32_t)(uint32_t)w1;
-            }
+            for (int s = 0; s < MAXS; ++s)
+                if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+            row = false;
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            bool row = has[u];
-            ull c0[MAXS], c1[MAXS];
-#pragma unroll
-            for (int s = 0; s < MAXS; ++s) {
-                c0[s] = 0;
-                c1[s] = 0;
-                if (row && s < p.n_st)
-                    contribution(p, p.st[s], raw[u][s], (vbits[u] >> s) & 1, (dfit[u] >> s) & 1,
-                                 p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, c0[s], c1[s]);
-            }
-            // Bit length of the largest |v| fed to an int64 SUM: decides
-            // whether a row-order prefix of some group could leave the i64
-            // range (then the exact row-order check runs after the query).
-            if (row && p.i64_bits) {
+        // Warp-level pre-aggregation of duplicate keys.
+        if (p.warp_agg) {
+            const uint32_t act = __ballot_sync(0xffffffffu, row);
+            uint32_t peers = 0;
+            if (row) peers = __match_any_sync(act, stored[u]);
+            const bool leader = row && (uint32_t)(__ffs(peers) - 1) == lane;
+            uint32_t others = leader ? (peers & ~(1u << lane)) : 0u;
+            const int rounds = __reduce_max_sync(0xffffffffu, (uint32_t)__popc(others));
+            for (int it = 0; it < rounds; ++it) {
+                int src = (int)lane;
+                if (others) {
+                    src = __ffs(others) - 1;
+                    others &= others - 1;
+                }
 #pragma unroll
                 for (int s = 0; s < MAXS; ++s) {
-                    if (s < p.n_st && p.st[s].kind == K_SUM_I64 && ((vbits[u] >> s) & 1)) {
-                        const ll v = (ll)raw[u][s];
-                        const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
-                        const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
-                        absbits = b > absbits ? b : absbits;
+                    if (s < NS) {
+                        const ull b0 = __shfl_sync(0xffffffffu, c0[s], src);
+                        const ull b1 = __shfl_sync(0xffffffffu, c1[s], src);
+                        if (leader && src != (int)lane) combine(skind<SP>(p, s), c0[s], c1[s], b0, b1);
                     }
                 }
             }
-            // Special groups: the NULL key and the key whose complement is 0.
-            const bool special = row && (knull[u] || stored[u] == 0);
-            if (special) {
-                const ull slot = (1ull << p.log2cap) + (knull[u] ? 1 : 0);
-                ull* w = p.gtab + slot * (ull)p.slot_words;
-                if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
+            row = leader;
+        }
+        if (!row) continue;
+        int sl = -1;
+        if (C) sl = s_find_insert(sk, p.smem_log2, stored[u]);
+        if (sl >= 0) {
+            ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
+            if (p.smem32) {
 #pragma unroll
                 for (int s = 0; s < MAXS; ++s)
-                    if (s < p.n_st) merge_words(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
-                row = false;
-            }
-            // Warp-level pre-aggregation of duplicate keys.
-            if (p.warp_agg) {
-                const uint32_t act = __ballot_sync(0xffffffffu, row);
-                uint32_t peers = 0;
-                if (row) peers = __match_any_sync(act, stored[u]);
-                const bool leader = row && (uint32_t)(__ffs(peers) - 1) == lane;
-                uint32_t others = leader ? (peers & ~(1u << lane)) : 0u;
-                const int rounds = __reduce_max_sync(0xffffffffu, (uint32_t)__popc(others));
-                for (int it = 0; it < rounds; ++it) {
-                    int src = (int)lane;
-                    if (others) {
-                        src = __ffs(others) - 1;
-                        others &= others - 1;
-                    }
-#pragma unroll
-                    for (int s = 0; s < MAXS; ++s) {
-                        if (s < p.n_st) {
-                            ull b0 = __shfl_sync(0xffffffffu, c0[s], src);
-                            ull b1 = __shfl_sync(0xffffffffu, c1[s], src);
-                            if (leader && src != (int)lane) combine(p.st[s].kind, c0[s], c1[s], b0, b1);
-                        }
-                    }
-                }
-                row = leader;
-            }
-            if (!row) continue;
-            int sl = -1;
-            if (C) sl = s_find_insert(sk, p.smem_log2, stored[u]);
-            if (sl >= 0) {
-                ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
-                if (p.smem32) {
-#pragma unroll
-                    for (int s = 0; s < MAXS; ++s)
-                        if (s < p.n_st) merge_words_s32(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
-                } else {
-#pragma unroll
-                    for (int s = 0; s < MAXS; ++s)
-                        if (s < p.n_st) merge_words(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
-                }
+                    if (s < NS) merge_words_s32(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
             } else {
-                int64_t g = g_find_insert(p, stored[u], inserts);
-                if (g >= 0) {
-                    ull* w = p.gtab + (ull)g * p.slot_words;
 #pragma unroll
-                    for (int s = 0; s < MAXS; ++s)
-                        if (s < p.n_st) merge_words(w + p.st[s].word, p.st[s].kind, c0[s], c1[s]);
-                }
+                for (int s = 0; s < MAXS; ++s)
+                    if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+            }
+        } else {
+            const int64_t g = g_find_insert(p, stored[u], inserts);
+            if (g >= 0) {
+                ull* w = p.gtab + (ull)g * p.slot_words;
+#pragma unroll
+                for (int s = 0; s < MAXS; ++s)
+                    if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
             }
         }
     }
 }
 
-// Per-tile occupancy accounting (call with the whole CTA): returns true once
-// the query's table must grow or spilled, so the CTA stops early.
-__device__ __forceinline__ bool gb_tile_epilogue(const GbParams& p, uint32_t& inserts, uint32_t* s_ins, int* s_stop) {
-    if (inserts) {
-        atomicAdd(s_ins, inserts);
-        inserts = 0;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        if (*s_ins) {
-            ull tot = atomicAdd(p.occupancy, (ull)*s_ins) + *s_ins;
-            *s_ins = 0;
+// Per-warp occupancy accounting after a tile (whole warp, no block barrier):
+// new keys are added to the query's counter in batches, and the warp learns
+// whether the query already flagged growth or a spill (then it stops).
+__device__ __forceinline__ bool gb_warp_epilogue(const GbParams& p, uint32_t& inserts, uint32_t& pending) {
+    pending += __reduce_add_sync(0xffffffffu, inserts);
+    inserts = 0;
+    const uint32_t batch = p.log2cap > 20 ? 256u : (p.log2cap > 12 ? (1u << (p.log2cap - 12)) : 1u);
+    uint32_t stop = 0;
+    if (lane_id() == 0) {
+        if (pending >= batch) {
+            const ull tot = atomicAdd(p.occupancy, (ull)pending) + pending;
             if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
         }
-        *s_stop = (*reinterpret_cast<volatile uint32_t*>(p.status) & (ST_FLAG_GROW | ST_FLAG_SPILL)) != 0;
+        stop = (*reinterpret_cast<volatile uint32_t*>(p.status) & (ST_FLAG_GROW | ST_FLAG_SPILL)) != 0;
     }
-    __syncthreads();
-    return *s_stop != 0;
+    if (pending >= batch) pending = 0;
+    return __shfl_sync(0xffffffffu, stop, 0) != 0;
+}
+
+// Adds a warp's not yet published key count to the query's counter.
+__device__ __forceinline__ void gb_warp_flush_pending(const GbParams& p, uint32_t& pending) {
+    if (lane_id() == 0 && pending) {
+        const ull tot = atomicAdd(p.occupancy, (ull)pending) + pending;
+        if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
+    }
+    pending = 0;
 }
 
 // Publishes the warp's largest |v| bit length for int64 SUMs (whole warp).
@@ -529,7 +574,7 @@ __device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk
     for (int i = threadIdx.x; i < C; i += blockDim.x) {
         const ull key = sk[i];
         if (key == 0) continue;
-        int64_t g = g_find_insert(p, key, inserts);
+        const int64_t g = g_find_insert(p, key, inserts);
         if (g < 0) continue;
         ull* w = p.gtab + (ull)g * p.slot_words;
         const ull* src = sw + (ull)i * SW - 1;
@@ -539,29 +584,27 @@ __device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk
         }
     }
     if (inserts) {
-        ull tot = atomicAdd(p.occupancy, (ull)inserts) + inserts;
+        const ull tot = atomicAdd(p.occupancy, (ull)inserts) + inserts;
         if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
     }
 }
 
-template <int U, int MAXS>
+template <int U, int MAXS, class SP>
 __global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbParams p) {
     extern __shared__ __align__(16) ull smem[];
-    __shared__ uint32_t s_ins;
-    __shared__ int s_stop;
     const int SW = p.slot_words - 1;
     const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
     ull* sk = smem;
     ull* sw = smem + C;
     for (int i = threadIdx.x; i < C * (SW + 1); i += blockDim.x) smem[i] = 0;
-    if (threadIdx.x == 0) { s_ins = 0; s_stop = 0; }
     __syncthreads();
     const uint64_t tile = (uint64_t)blockDim.x * U;
-    uint32_t inserts = 0, absbits = 0;
+    uint32_t inserts = 0, pending = 0, absbits = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * tile; base < p.n_rows; base += (uint64_t)gridDim.x * tile) {
-        gb_process_tile<U, MAXS>(p, sk, sw, C, base, inserts, absbits);
-        if (gb_tile_epilogue(p, inserts, &s_ins, &s_stop)) return;
+        gb_process_tile<U, MAXS, SP>(p, sk, sw, C, base, inserts, absbits);
+        if (gb_warp_epilogue(p, inserts, pending)) break;
     }
+    gb_warp_flush_pending(p, pending);
     gb_flush_absbits(p, absbits);
     __syncthreads();
     gb_flush_shared(p, sk, sw, C);
@@ -802,15 +845,6 @@ __global__ void __launch_bounds__(1024) gb_small_final_kernel(const GbFinal* fin
     for (uint64_t o = threadIdx.x; o < lim; o += blockDim.x) emit_group(f, o, o < G ? slot[o] : cap + 1);
 }
 
-template <int U, int MAXS>
-bolt_status launch_agg(bolt_ctx* ctx, const GbPlan& pl, cudaStream_t s, size_t smem) {
-    auto kfn = gb_agg_kernel<U, MAXS>;
-    BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kfn<<<pl.grid, pl.block, smem, s>>>(pl.prm);
-    ctx->last_launches++;
-    return BOLT_OK;
-}
-
 // ---------------------------------------------------------------------------
 // Exact row-order check of int64 SUM (checked_group_sum, groupby.rs:1775):
 // only run when some group's partial sums could leave the i64 range.
@@ -893,34 +927,31 @@ __global__ void __launch_bounds__(256) gb_prefix_check_kernel(const __grid_const
     }
 }
 
-// Persistent multi-query aggregation: work items are (query, tile of
-// blockDim.x * U rows) handed out in order from one counter. A CTA keeps one
-// query's shared table while its items stay on that query and merges it into
-// that query's global table when it moves on. Each query has its own table,
-// occupancy and status words, so one query's spill never touches another's.
-template <int U, int MAXS>
+// Persistent multi-query aggregation: work items are (query, run of
+// item_tiles tiles of blockDim.x * U rows) handed out in order from one
+// counter. A CTA keeps one query's shared table while its items stay on that
+// query and merges it into that query's global table when it moves on. Each
+// query has its own table, occupancy and status words, so one query's spill
+// never touches another's. One block barrier per item (the hand-out).
+template <int U, int MAXS, class SP>
 __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms, const uint32_t* begins, int nq,
-                                                           uint32_t total_items, uint32_t* counter) {
+                                                           uint32_t total_items, uint32_t item_tiles,
+                                                           uint32_t* counter) {
     extern __shared__ __align__(16) ull smem[];
     __shared__ __align__(16) GbParams p;
-    __shared__ uint32_t s_item;
-    __shared__ uint32_t s_ins;
-    __shared__ int s_stop;
-    int cur = -1;
+    __shared__ uint32_t s_item[2];  // alternating: a slot is rewritten only after everyone read it
+    int cur = -1, stopped = -1;
     int C = 0;
-    uint32_t inserts = 0, absbits = 0;
-    if (threadIdx.x == 0) {
-        s_ins = 0;
-        s_stop = 0;
-    }
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+    uint32_t inserts = 0, pending = 0, absbits = 0;
+    for (uint32_t it = 0;; ++it) {
+        if (threadIdx.x == 0) s_item[it & 1] = atomicAdd(counter, 1u);
         __syncthreads();
-        const uint32_t item = s_item;
+        const uint32_t item = s_item[it & 1];
         if (item >= total_items) break;
         const int q = query_of(begins, nq, item);
         if (q != cur) {
             if (cur >= 0) {
+                gb_warp_flush_pending(p, pending);
                 gb_flush_absbits(p, absbits);
                 gb_flush_shared(p, smem, smem + C, C);
                 __syncthreads();
@@ -928,23 +959,61 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
             const int4* src = reinterpret_cast<const int4*>(prms + q);
             int4* dst = reinterpret_cast<int4*>(&p);
             for (int i = threadIdx.x; i < (int)(sizeof(GbParams) / 16); i += blockDim.x) dst[i] = src[i];
-            if (threadIdx.x == 0) s_stop = 0;
             __syncthreads();
             C = p.smem_log2 ? (1 << p.smem_log2) : 0;
             for (int i = threadIdx.x; i < C * p.slot_words; i += blockDim.x) smem[i] = 0;
             __syncthreads();
             cur = q;
-        } else if (s_stop) {
-            __syncthreads();
-            continue;  // the query already flagged growth; the host re-runs it
         }
-        const uint64_t base = (uint64_t)(item - begins[q]) * blockDim.x * U;
-        gb_process_tile<U, MAXS>(p, smem, smem + C, C, base, inserts, absbits);
-        gb_tile_epilogue(p, inserts, &s_ins, &s_stop);
+        if (stopped == q) continue;  // the query already flagged growth; the host re-runs it
+        const uint64_t tile = (uint64_t)blockDim.x * U;
+        const uint64_t first = (uint64_t)(item - begins[q]) * item_tiles * tile;
+        for (uint32_t t = 0; t < item_tiles; ++t) {
+            const uint64_t base = first + (uint64_t)t * tile;
+            if (base >= p.n_rows) break;
+            gb_process_tile<U, MAXS, SP>(p, smem, smem + C, C, base, inserts, absbits);
+            if (gb_warp_epilogue(p, inserts, pending)) {
+                stopped = q;
+                break;
+            }
+        }
     }
     if (cur >= 0) {
+        gb_warp_flush_pending(p, pending);
         gb_flush_absbits(p, absbits);
+        __syncthreads();
         gb_flush_shared(p, smem, smem + C, C);
+    }
+}
+
+using AggKernel = void (*)(GbParams);
+using BatchKernel = void (*)(const GbParams*, const uint32_t*, int, uint32_t, uint32_t, uint32_t*);
+
+// Kernel instantiation for a compiled state layout (gb_spec_of); the generic
+// loop handles up to 4 states at 4 rows per thread or 8 states at 2.
+AggKernel agg_kernel_for(int spec, int n_st) {
+    switch (spec) {
+    case 1: return gb_agg_kernel<4, 4, Spec1>;
+    case 2: return gb_agg_kernel<4, 4, Spec2>;
+    case 3: return gb_agg_kernel<4, 2, Spec3>;
+    case 4: return gb_agg_kernel<4, 2, Spec4>;
+    case 5: return gb_agg_kernel<4, 2, Spec5>;
+    case 6: return gb_agg_kernel<4, 1, Spec6>;
+    case 7: return gb_agg_kernel<4, 2, Spec7>;
+    default: return n_st <= 4 ? gb_agg_kernel<4, 4, SpecGeneric> : gb_agg_kernel<2, 8, SpecGeneric>;
+    }
+}
+
+BatchKernel batch_kernel_for(int spec, int max_st) {
+    switch (spec) {
+    case 1: return gb_batch_agg_kernel<4, 4, Spec1>;
+    case 2: return gb_batch_agg_kernel<4, 4, Spec2>;
+    case 3: return gb_batch_agg_kernel<4, 2, Spec3>;
+    case 4: return gb_batch_agg_kernel<4, 2, Spec4>;
+    case 5: return gb_batch_agg_kernel<4, 2, Spec5>;
+    case 6: return gb_batch_agg_kernel<4, 1, Spec6>;
+    case 7: return gb_batch_agg_kernel<4, 2, Spec7>;
+    default: return max_st <= 4 ? gb_batch_agg_kernel<4, 4, SpecGeneric> : gb_batch_agg_kernel<2, 8, SpecGeneric>;
     }
 }
 
@@ -953,6 +1022,28 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
 // ---------------------------------------------------------------------------
 // Planning
 // ---------------------------------------------------------------------------
+namespace {
+template <class SP>
+bool spec_matches(const StateDesc* st, int n) {
+    if (n != SP::n) return false;
+    for (int s = 0; s < n; ++s)
+        if (st[s].kind != SP::kind(s)) return false;
+    return true;
+}
+}  // namespace
+
+// Which compiled row loop serves these (canonically ordered) states.
+int gb_spec_of(const StateDesc* st, int n) {
+    if (spec_matches<Spec1>(st, n)) return 1;
+    if (spec_matches<Spec2>(st, n)) return 2;
+    if (spec_matches<Spec3>(st, n)) return 3;
+    if (spec_matches<Spec4>(st, n)) return 4;
+    if (spec_matches<Spec5>(st, n)) return 5;
+    if (spec_matches<Spec6>(st, n)) return 6;
+    if (spec_matches<Spec7>(st, n)) return 7;
+    return 0;
+}
+
 uint64_t gb_shape_key(const GbParams& p, uint64_t n_rows, uint64_t groups_hint) {
     uint64_t h = 1469598103934665603ull;
     auto mix = [&](uint64_t v) {
@@ -1109,6 +1200,33 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         g.out = out->aggs[a].data;
         g.out_valid = out->aggs[a].validity;
     }
+    // Canonical state order (COUNT, SUMs, MAX, MIN, the rest; stable), so the
+    // common layouts hit a row loop compiled for them.
+    {
+        auto rank = [](int k) {
+            return k == K_COUNT ? 0 : (k == K_SUM_I32 || k == K_SUM_I64 || k == K_SUM_FX || k == K_SUM_D64) ? 1
+                 : k == K_MAX_ORD ? 2 : k == K_MIN_ORD ? 3 : 4;
+        };
+        int order[GB_MAX_STATES], where[GB_MAX_STATES];
+        for (int s = 0; s < n_st; ++s) order[s] = s;
+        std::stable_sort(order, order + n_st, [&](int a, int b) { return rank(p.st[a].kind) < rank(p.st[b].kind); });
+        StateDesc sorted[GB_MAX_STATES];
+        word = 1;
+        for (int i = 0; i < n_st; ++i) {
+            sorted[i] = p.st[order[i]];
+            sorted[i].word = word;
+            word += sorted[i].nwords;
+            where[order[i]] = i;
+        }
+        for (int i = 0; i < n_st; ++i) p.st[i] = sorted[i];
+        for (int a = 0; a < d->n_aggs; ++a) {
+            AggOut& g = f.agg[a];
+            if (g.sum_state >= 0) g.sum_state = where[g.sum_state];
+            if (g.cnt_state >= 0) g.cnt_state = where[g.cnt_state];
+            if (g.mm_state >= 0) g.mm_state = where[g.mm_state];
+        }
+        p.spec = gb_spec_of(p.st, n_st);
+    }
     p.n_st = n_st;
     p.slot_words = word;
     f.slot_words = word;
@@ -1183,16 +1301,15 @@ uint64_t gb_plan_scratch(const GbPlan& pl) {
 
 namespace {
 
-template <int U, int MAXS>
-bolt_status launch_batch_agg(bolt_ctx* ctx, cudaStream_t s, const GbParams* d_prms, const uint32_t* d_begins, int nq,
-                             uint32_t items, uint32_t* counter, size_t smem, int block) {
-    auto kfn = gb_batch_agg_kernel<U, MAXS>;
+bolt_status launch_batch_agg(bolt_ctx* ctx, cudaStream_t s, BatchKernel kfn, const GbParams* d_prms,
+                             const uint32_t* d_begins, int nq, uint32_t items, uint32_t item_tiles, uint32_t* counter,
+                             size_t smem, int block) {
     BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, items);
-    kfn<<<grid, block, smem, s>>>(d_prms, d_begins, nq, items, counter);
+    kfn<<<grid, block, smem, s>>>(d_prms, d_begins, nq, items, item_tiles, counter);
     ctx->last_launches++;
     return BOLT_OK;
 }
@@ -1241,36 +1358,37 @@ bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t
         const size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
         const uint64_t tile = (uint64_t)pl->block * pl->u;
         const uint64_t tiles = (p.n_rows + tile - 1) / tile;
+        const AggKernel kfn = agg_kernel_for(p.spec, p.n_st);
         int per_sm = 1;
-        cudaError_t e;
-        if (pl->u == 4) {
-            BOLT_CUDA(ctx, cudaFuncSetAttribute(gb_agg_kernel<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb_agg_kernel<4, 4>, pl->block, smem);
-        } else {
-            BOLT_CUDA(ctx, cudaFuncSetAttribute(gb_agg_kernel<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb_agg_kernel<2, 8>, pl->block, smem);
-        }
-        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+        BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, pl->block, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
         uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
         if (pl->grid > 0) grid = std::min<uint64_t>(grid, (uint64_t)pl->grid);
         pl->grid = (int)grid;
         if (p.n_rows > 0) {
             kernel_mark_begin(ctx, flags, s);
-            bolt_status st = pl->u == 4 ? launch_agg<4, 4>(ctx, *pl, s, smem) : launch_agg<2, 8>(ctx, *pl, s, smem);
+            kfn<<<pl->grid, pl->block, smem, s>>>(p);
+            ctx->last_launches++;
             kernel_mark_end(ctx, flags, s);
-            if (st != BOLT_OK) return st;
         }
     } else {
-        int u = 4;
+        // One compiled row loop for the whole batch: the queries' common
+        // layout, else the generic loop.
+        int u = 4, max_st = 0, spec = pls[0]->prm.spec;
         size_t smem = 0;
         for (int q = 0; q < nq; ++q) {
-            if (pls[q]->prm.n_st > 4) u = 2;
+            max_st = std::max(max_st, (int)pls[q]->prm.n_st);
+            if (pls[q]->prm.spec != spec) spec = 0;
             smem = std::max<size_t>(smem, (size_t)pls[q]->smem_entries * 8 * (size_t)pls[q]->prm.slot_words);
         }
+        if (spec == 0 && max_st > 4) u = 2;
+        const BatchKernel kfn = batch_kernel_for(spec, max_st);
+        const uint32_t item_tiles = 4;
         std::vector<GbParams> prms(nq);
         std::vector<uint32_t> begins(nq + 1);
         uint64_t items = 0;
-        const uint64_t tile = 512ull * u;
+        const uint64_t tile = 512ull * u * item_tiles;
         for (int q = 0; q < nq; ++q) {
             prms[q] = pls[q]->prm;
             begins[q] = (uint32_t)items;
@@ -1288,8 +1406,7 @@ bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t
         BOLT_CUDA(ctx, cudaMemsetAsync(counter, 0, 4, s));
         if (items) {
             kernel_mark_begin(ctx, flags, s);
-            st = u == 4 ? launch_batch_agg<4, 4>(ctx, s, d_prms, d_begins, nq, (uint32_t)items, counter, smem, 512)
-                        : launch_batch_agg<2, 8>(ctx, s, d_prms, d_begins, nq, (uint32_t)items, counter, smem, 512);
+            st = launch_batch_agg(ctx, s, kfn, d_prms, d_begins, nq, (uint32_t)items, item_tiles, counter, smem, 512);
             kernel_mark_end(ctx, flags, s);
             if (st != BOLT_OK) return st;
         }

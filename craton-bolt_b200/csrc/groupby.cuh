@@ -77,7 +77,7 @@ struct alignas(16) GbParams {
     int32_t fx_e;
     int32_t warp_agg;
     int32_t smem32;      // shared tier merges with native 32-bit atomics
-    int32_t pad0;
+    int32_t spec;        // compiled row-loop layout (gb_spec_of), 0 = generic
     uint32_t* status;
     ull* occupancy;
     ull grow_limit;
@@ -137,6 +137,8 @@ struct GbPlan {
 // Key of a query shape for the autotuning cache: key / predicate / state
 // layout plus the row and group counts rounded to powers of two.
 uint64_t gb_shape_key(const GbParams& p, uint64_t n_rows, uint64_t groups_hint);
+// Compiled row-loop layout serving these canonically ordered states (0 = generic).
+int gb_spec_of(const StateDesc* st, int n);
 
 // Plan modes selected after a flagged first attempt.
 constexpr int GB_MODE_F64_ATOMIC = 1;  // f64 SUM with plain atomics (non-finite / huge inputs)
