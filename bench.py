@@ -127,8 +127,12 @@ class ClockSampler:
 
             if device_index < 0:
                 raise RuntimeError("clock sampling disabled")
-            bus = torch.cuda.get_device_properties(device_index).pci_bus_id
-            self.bus_tail = bus.upper()[-7:]  # "1B:00.0"
+            props = torch.cuda.get_device_properties(device_index)
+            bus = props.pci_bus_id
+            if isinstance(bus, str):
+                self.bus_tail = bus.upper()[-7:]  # "1B:00.0"
+            else:  # integer bus / device numbers
+                self.bus_tail = f"{int(bus):02X}:{int(getattr(props, 'pci_device_id', 0)):02X}.0"
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", str(period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -355,11 +359,16 @@ def w_groupby_filtered(c: Ctx):
     pq = c.eng.prepare_groupby(dev, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], groups_hint=a.groups_hint,
                                out_cap=max(2 * a.groups_hint, 1 << 20))
     tuned = None
-    if not a.no_tune:
+    if a.tuning:
+        c.eng.load_tuning(a.tuning)
+        tuned = {"loaded": os.path.basename(a.tuning)}
+    elif not a.no_tune:
         progress("autotuning")
         best = c.eng.autotune_groupby(pq)
         tuned = {"best_ms": best}
         progress(f"autotuned: {best:.3f} ms")
+    if a.save_tuning:
+        c.eng.save_tuning(a.save_tuning)
     call = PreparedCall(c, pq)
     ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
     n_groups = int(call.ng.item())
@@ -749,6 +758,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the GROUP BY autotuner")
+    ap.add_argument("--tuning", default=None, help="load GROUP BY launch choices from this file instead of tuning")
+    ap.add_argument("--save-tuning", default=None, help="write the GROUP BY launch choices to this file")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -46,7 +46,7 @@ struct bolt_ctx {
     StageUse stage_use[STAGE_SLOTS] = {};
     uint32_t stage_next = 0;
     // Autotuned GROUP BY launch choices per query shape (see gb_shape_key).
-    struct GbTune { int32_t block, smem_shift, warp_agg, load_shift, smem32; double ms; };
+    struct GbTune { int32_t block, smem_shift, warp_agg, load_shift, smem_fill; double ms; };  // smem_fill in eighths
     std::unordered_map<uint64_t, GbTune> tune;
 };
 

@@ -201,77 +201,21 @@ __device__ __forceinline__ void merge_words(ull* w, int kind, ull c0, ull c1) {
     }
 }
 
-// ---- shared-memory merge built from native 32-bit atomics -----------------
-// 64-bit add / max on shared memory have no single native instruction; a
-// compiler-generated compare-and-swap loop serialises badly when many warps
-// hit one hot group. These variants use native 32-bit atomicAdd on the
-// words' halves with the carry of each limb computed from that atomic's own
-// old value (so concurrent adds still sum exactly, modulo the word width),
-// and MIN/MAX read first and CAS only when the new value would win.
-__device__ __forceinline__ void s32_add64(ull* w, ull x) {
-    uint32_t* p = reinterpret_cast<uint32_t*>(w);
-    const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32);
-    uint32_t carry = 0;
-    if (xl) {
-        const uint32_t old = atomicAdd(p, xl);
-        carry = (uint32_t)(((ull)old + xl) >> 32);
-    }
-    const uint32_t h = xh + carry;  // modulo 2^32, as the word is
-    if (h) atomicAdd(p + 1, h);
-}
-
-// 128-bit add of (x0 low, x1 high) into w[0..1], limb by limb.
-__device__ __forceinline__ void s32_add128(ull* w, ull x0, ull x1) {
-    uint32_t* p = reinterpret_cast<uint32_t*>(w);
-    const uint32_t x[4] = {(uint32_t)x0, (uint32_t)(x0 >> 32), (uint32_t)x1, (uint32_t)(x1 >> 32)};
-    uint32_t carry = 0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const ull add = (ull)x[i] + carry;
-        if (add == 0) {
-            carry = 0;
-            continue;
-        }
-        const uint32_t a32 = (uint32_t)add;
-        if (i == 3) {
-            if (a32) atomicAdd(p + 3, a32);
-            break;
-        }
-        if (a32 == 0) {  // add == 2^32: this limb unchanged, carry one out
-            carry = 1;
-            continue;
-        }
-        const uint32_t old = atomicAdd(p + i, a32);
-        carry = (uint32_t)(((ull)old + a32) >> 32);
-    }
-}
-
-__device__ __forceinline__ void s32_max64(ull* w, ull x) {
-    ull cur = *reinterpret_cast<volatile ull*>(w);
-    while (x > cur) {
-        const ull old = atomicCAS(w, cur, x);
-        if (old == cur) break;
-        cur = old;
-    }
-}
-
-__device__ __forceinline__ void merge_words_s32(ull* w, int kind, ull c0, ull c1) {
+// Row-path merge into the shared-memory tier. Shared 64-bit atomic add and
+// max are compare-and-swap loops that serialise when lanes of a warp (or
+// several warps) hit one hot group, while 32-bit reductions are native and
+// combine same-address lanes. So COUNT accumulates in the low 32 bits of its
+// word (exact while a CTA's table sees fewer than 2^32 rows: cnt32), and
+// MIN / MAX read the word first and only CAS when the row would win, which
+// for a hot group is rarely after its first few rows.
+__device__ __forceinline__ void merge_words_smem(ull* w, int kind, ull c0, ull c1, bool cnt32) {
     if ((c0 | c1) == 0) return;
-    switch (kind) {
-    case K_COUNT:
-    case K_SUM_I32: s32_add64(w, c0); break;
-    case K_SUM_I64:
-    case K_SUM_D64:
-        if (c0) s32_add64(w, c0);
-        if (c1) s32_add64(w + 1, c1);
-        break;
-    case K_SUM_FX: s32_add128(w, c0, c1); break;
-    case K_SUM_D128:
-        s32_add128(w, c0, c1 & 0xFFFFFFFFull);
-        if ((ll)c1 >> 32) s32_add64(w + 2, (ull)((ll)c1 >> 32));
-        break;
-    case K_SUM_FATOM: atomicAdd(reinterpret_cast<double*>(w), __longlong_as_double((ll)c0)); break;
-    default: s32_max64(w, c0); break;
+    if (kind == K_COUNT && cnt32) {
+        atomicAdd(reinterpret_cast<uint32_t*>(w), (uint32_t)c0);
+    } else if (kind == K_MAX_ORD || kind == K_MIN_ORD) {
+        if (c0 > *reinterpret_cast<volatile ull*>(w)) atomicMax(w, c0);
+    } else {
+        merge_words(w, kind, c0, c1);
     }
 }
 
@@ -318,7 +262,12 @@ __device__ __forceinline__ int64_t g_find_insert(const GbParams& p, ull stored, 
     return -1;
 }
 
-__device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored) {
+// Shared-tier find-or-insert. New keys are admitted only while the table
+// holds fewer than `limit` keys (counted in *fill), so the table never fills
+// up: a key that is absent meets an empty slot after a few probes and goes to
+// the global table, instead of scanning the whole probe window. The first
+// keys a CTA meets are admitted, which under skew are the frequent ones.
+__device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored, uint32_t* fill, uint32_t limit) {
     const uint32_t mask = (1u << log2) - 1;
     uint32_t h = (uint32_t)((stored * HASH_S) >> (64 - log2));
     volatile ull* vk = sk;
@@ -326,8 +275,13 @@ __device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored) {
         ull k = vk[h];
         if (k == stored) return (int)h;
         if (k == 0) {
+            if (*reinterpret_cast<volatile uint32_t*>(fill) >= limit) return -1;
             ull old = atomicCAS(&sk[h], 0ull, stored);
-            if (old == 0 || old == stored) return (int)h;
+            if (old == 0) {
+                atomicAdd(fill, 1u);
+                return (int)h;
+            }
+            if (old == stored) return (int)h;
         }
         h = (h + 1) & mask;
     }
@@ -379,8 +333,8 @@ __device__ __forceinline__ int snum(const GbParams& p) {
 // load, filter, key, pre-aggregate and fold into the shared or global table.
 // `sk` / `sw` are the shared table's keys and state words (C slots, C may be 0).
 template <int U, int MAXS, class SP>
-__device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull* sw, int C, uint64_t base,
-                                                uint32_t& inserts, uint32_t& absbits) {
+__device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull* sw, int C, uint32_t* fill,
+                                                uint64_t base, uint32_t& inserts, uint32_t& absbits) {
     const int SW = p.slot_words - 1;
     const uint32_t lane = lane_id();
     const uint64_t n = p.n_rows;
@@ -443,90 +397,99 @@ __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull*
             stored[u] = ~(ull)(ll)(int32_t)(uint32_t)w1;
         }
     }
-#pragma unroll
+    // Rows are folded one at a time in a rolled loop (one copy of the code,
+    // which keeps the kernel inside the instruction cache): row u sits in
+    // slot 0 and the later rows move down one slot after each iteration.
+#pragma unroll 1
     for (int u = 0; u < U; ++u) {
-        bool row = has[u];
-        ull c0[MAXS], c1[MAXS];
-#pragma unroll
-        for (int s = 0; s < MAXS; ++s) {
-            c0[s] = 0;
-            c1[s] = 0;
-            if (row && s < NS)
-                contribution(p, p.st[s], skind<SP>(p, s), raw[u][s], (vbits[u] >> s) & 1, (dfit[u] >> s) & 1,
-                             p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, c0[s], c1[s]);
-        }
-        // Bit length of the largest |v| fed to an int64 SUM: decides whether
-        // a row-order prefix of some group could leave the i64 range (then
-        // the exact row-order check runs after the query).
-        if (row && p.i64_bits) {
+        do {
+            bool row = has[0];
+            ull c0[MAXS], c1[MAXS];
 #pragma unroll
             for (int s = 0; s < MAXS; ++s) {
-                if (s < NS && skind<SP>(p, s) == K_SUM_I64 && ((vbits[u] >> s) & 1)) {
-                    const ll v = (ll)raw[u][s];
-                    const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
-                    const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
-                    absbits = b > absbits ? b : absbits;
-                }
+                c0[s] = 0;
+                c1[s] = 0;
+                if (row && s < NS)
+                    contribution(p, p.st[s], skind<SP>(p, s), raw[0][s], (vbits[0] >> s) & 1, (dfit[0] >> s) & 1,
+                                 p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, c0[s], c1[s]);
             }
-        }
-        // Special groups: the NULL key and the key whose complement is 0.
-        const bool special = row && (knull[u] || stored[u] == 0);
-        if (special) {
-            const ull slot = (1ull << p.log2cap) + (knull[u] ? 1 : 0);
-            ull* w = p.gtab + slot * (ull)p.slot_words;
-            if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
-#pragma unroll
-            for (int s = 0; s < MAXS; ++s)
-                if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
-            row = false;
-        }
-        // Warp-level pre-aggregation of duplicate keys.
-        if (p.warp_agg) {
-            const uint32_t act = __ballot_sync(0xffffffffu, row);
-            uint32_t peers = 0;
-            if (row) peers = __match_any_sync(act, stored[u]);
-            const bool leader = row && (uint32_t)(__ffs(peers) - 1) == lane;
-            uint32_t others = leader ? (peers & ~(1u << lane)) : 0u;
-            const int rounds = __reduce_max_sync(0xffffffffu, (uint32_t)__popc(others));
-            for (int it = 0; it < rounds; ++it) {
-                int src = (int)lane;
-                if (others) {
-                    src = __ffs(others) - 1;
-                    others &= others - 1;
-                }
+            // Bit length of the largest |v| fed to an int64 SUM: decides whether
+            // a row-order prefix of some group could leave the i64 range (then
+            // the exact row-order check runs after the query).
+            if (row && p.i64_bits) {
 #pragma unroll
                 for (int s = 0; s < MAXS; ++s) {
-                    if (s < NS) {
-                        const ull b0 = __shfl_sync(0xffffffffu, c0[s], src);
-                        const ull b1 = __shfl_sync(0xffffffffu, c1[s], src);
-                        if (leader && src != (int)lane) combine(skind<SP>(p, s), c0[s], c1[s], b0, b1);
+                    if (s < NS && skind<SP>(p, s) == K_SUM_I64 && ((vbits[0] >> s) & 1)) {
+                        const ll v = (ll)raw[0][s];
+                        const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
+                        const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
+                        absbits = b > absbits ? b : absbits;
                     }
                 }
             }
-            row = leader;
-        }
-        if (!row) continue;
-        int sl = -1;
-        if (C) sl = s_find_insert(sk, p.smem_log2, stored[u]);
-        if (sl >= 0) {
-            ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
-            if (p.smem32) {
+            // Special groups: the NULL key and the key whose complement is 0.
+            const bool special = row && (knull[0] || stored[0] == 0);
+            if (special) {
+                const ull slot = (1ull << p.log2cap) + (knull[0] ? 1 : 0);
+                ull* w = p.gtab + slot * (ull)p.slot_words;
+                if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
 #pragma unroll
                 for (int s = 0; s < MAXS; ++s)
-                    if (s < NS) merge_words_s32(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+                    if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+                row = false;
+            }
+            // Warp-level pre-aggregation of duplicate keys.
+            if (p.warp_agg) {
+                const uint32_t act = __ballot_sync(0xffffffffu, row);
+                uint32_t peers = 0;
+                if (row) peers = __match_any_sync(act, stored[0]);
+                const bool leader = row && (uint32_t)(__ffs(peers) - 1) == lane;
+                uint32_t others = leader ? (peers & ~(1u << lane)) : 0u;
+                const int rounds = __reduce_max_sync(0xffffffffu, (uint32_t)__popc(others));
+                for (int it = 0; it < rounds; ++it) {
+                    int src = (int)lane;
+                    if (others) {
+                        src = __ffs(others) - 1;
+                        others &= others - 1;
+                    }
+#pragma unroll
+                    for (int s = 0; s < MAXS; ++s) {
+                        if (s < NS) {
+                            const ull b0 = __shfl_sync(0xffffffffu, c0[s], src);
+                            const ull b1 = __shfl_sync(0xffffffffu, c1[s], src);
+                            if (leader && src != (int)lane) combine(skind<SP>(p, s), c0[s], c1[s], b0, b1);
+                        }
+                    }
+                }
+                row = leader;
+            }
+            if (!row) continue;
+            int sl = -1;
+            if (C) sl = s_find_insert(sk, p.smem_log2, stored[0], fill, p.smem_fill);
+            if (sl >= 0) {
+                ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
+#pragma unroll
+                for (int s = 0; s < MAXS; ++s)
+                    if (s < NS) merge_words_smem(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s], p.cnt32);
             } else {
+                const int64_t g = g_find_insert(p, stored[0], inserts);
+                if (g >= 0) {
+                    ull* w = p.gtab + (ull)g * p.slot_words;
 #pragma unroll
-                for (int s = 0; s < MAXS; ++s)
-                    if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+                    for (int s = 0; s < MAXS; ++s)
+                        if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+                }
             }
-        } else {
-            const int64_t g = g_find_insert(p, stored[u], inserts);
-            if (g >= 0) {
-                ull* w = p.gtab + (ull)g * p.slot_words;
+        } while (0);
 #pragma unroll
-                for (int s = 0; s < MAXS; ++s)
-                    if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
-            }
+        for (int v = 0; v + 1 < U; ++v) {
+            has[v] = has[v + 1];
+            knull[v] = knull[v + 1];
+            stored[v] = stored[v + 1];
+            vbits[v] = vbits[v + 1];
+            dfit[v] = dfit[v + 1];
+#pragma unroll
+            for (int s = 0; s < MAXS; ++s) raw[v][s] = raw[v + 1][s];
         }
     }
 }
@@ -590,18 +553,20 @@ __device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk
 }
 
 template <int U, int MAXS, class SP>
-__global__ void __launch_bounds__(512) gb_agg_kernel(const __grid_constant__ GbParams p) {
+__global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_agg_kernel(const __grid_constant__ GbParams p) {
     extern __shared__ __align__(16) ull smem[];
+    __shared__ uint32_t s_fill;
     const int SW = p.slot_words - 1;
     const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
     ull* sk = smem;
     ull* sw = smem + C;
     for (int i = threadIdx.x; i < C * (SW + 1); i += blockDim.x) smem[i] = 0;
+    if (threadIdx.x == 0) s_fill = 0;
     __syncthreads();
     const uint64_t tile = (uint64_t)blockDim.x * U;
     uint32_t inserts = 0, pending = 0, absbits = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * tile; base < p.n_rows; base += (uint64_t)gridDim.x * tile) {
-        gb_process_tile<U, MAXS, SP>(p, sk, sw, C, base, inserts, absbits);
+        gb_process_tile<U, MAXS, SP>(p, sk, sw, C, &s_fill, base, inserts, absbits);
         if (gb_warp_epilogue(p, inserts, pending)) break;
     }
     gb_warp_flush_pending(p, pending);
@@ -934,12 +899,13 @@ __global__ void __launch_bounds__(256) gb_prefix_check_kernel(const __grid_const
 // query has its own table, occupancy and status words, so one query's spill
 // never touches another's. One block barrier per item (the hand-out).
 template <int U, int MAXS, class SP>
-__global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms, const uint32_t* begins, int nq,
+__global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_batch_agg_kernel(const GbParams* prms, const uint32_t* begins, int nq,
                                                            uint32_t total_items, uint32_t item_tiles,
                                                            uint32_t* counter) {
     extern __shared__ __align__(16) ull smem[];
     __shared__ __align__(16) GbParams p;
     __shared__ uint32_t s_item[2];  // alternating: a slot is rewritten only after everyone read it
+    __shared__ uint32_t s_fill;
     int cur = -1, stopped = -1;
     int C = 0;
     uint32_t inserts = 0, pending = 0, absbits = 0;
@@ -962,6 +928,7 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
             __syncthreads();
             C = p.smem_log2 ? (1 << p.smem_log2) : 0;
             for (int i = threadIdx.x; i < C * p.slot_words; i += blockDim.x) smem[i] = 0;
+            if (threadIdx.x == 0) s_fill = 0;
             __syncthreads();
             cur = q;
         }
@@ -971,7 +938,7 @@ __global__ void __launch_bounds__(512) gb_batch_agg_kernel(const GbParams* prms,
         for (uint32_t t = 0; t < item_tiles; ++t) {
             const uint64_t base = first + (uint64_t)t * tile;
             if (base >= p.n_rows) break;
-            gb_process_tile<U, MAXS, SP>(p, smem, smem + C, C, base, inserts, absbits);
+            gb_process_tile<U, MAXS, SP>(p, smem, smem + C, C, &s_fill, base, inserts, absbits);
             if (gb_warp_epilogue(p, inserts, pending)) {
                 stopped = q;
                 break;
@@ -1241,7 +1208,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
 
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
     pl->shape = gb_shape_key(p, n, d->groups_hint);
-    bolt_ctx::GbTune tn{512, 0, 1, 1, 1, 0.0};
+    bolt_ctx::GbTune tn{512, 1, 0, 2, 4, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
@@ -1265,7 +1232,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     p.fx_e = 126 - 32 - ceil_log2_u64(n + 1);
     f.fx_e = p.fx_e;
     p.warp_agg = tn.warp_agg;
-    p.smem32 = tn.smem32;
+    // A CTA's shared table sees at most n rows: COUNT fits its low 32 bits.
+    p.cnt32 = n < 0xFFFFFFFFull ? 1 : 0;
     for (int s = 0; s < n_st; ++s)
         if (p.st[s].kind == K_SUM_D128) p.warp_agg = 0;  // D128 partials do not combine in registers
 
@@ -1283,6 +1251,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         else if (sl) sl = std::max(sl - tn.smem_shift, 6);
     }
     p.smem_log2 = sl;
+    p.smem_fill = sl ? (uint32_t)(((1ull << sl) * (uint64_t)tn.smem_fill) / 8) : 0;
     pl->smem_entries = sl ? (1 << sl) : 0;
     pl->u = n_st <= 4 ? 4 : 2;
     pl->block = tn.block;
@@ -1710,11 +1679,11 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
         for (int smem_shift : {0, 1, 8})
             for (int warp_agg : {0, 1})
                 for (int load_shift : {1, 2})
-                    for (int smem32 : {0, 1}) {
-                        if (smem_shift == 8 && smem32) continue;  // no shared tier: smem32 is moot
-                        cands.push_back({block, smem_shift, warp_agg, load_shift, smem32, 0.0});
+                    for (int smem_fill : {4, 6}) {
+                        if (smem_shift == 8 && smem_fill != 4) continue;  // no shared tier: the fill is moot
+                        cands.push_back({block, smem_shift, warp_agg, load_shift, smem_fill, 0.0});
                     }
-    bolt_ctx::GbTune best{512, 0, 1, 1, 1, 1e30};
+    bolt_ctx::GbTune best{512, 1, 0, 2, 4, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
     for (auto& c : cands) {
@@ -1744,8 +1713,8 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             if (rep > 0) tot += ms;  // first repetition warms up
         }
         if (verbose)
-            std::fprintf(stderr, "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem32=%d -> %s%.4f ms\n",
-                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem32, ok ? "" : "(flagged) ", tot / 2);
+            std::fprintf(stderr, "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem_fill=%d/8 -> %s%.4f ms\n",
+                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem_fill, ok ? "" : "(flagged) ", tot / 2);
         if (ok && tot / 2 < best.ms) {
             best = c;
             best.ms = tot / 2;
@@ -1763,7 +1732,7 @@ extern "C" bolt_status bolt_ctx_tuning_save(const bolt_ctx* ctx, const char* pat
     if (!fp) return BOLT_ERR_INVALID;
     for (const auto& kv : ctx->tune)
         std::fprintf(fp, "%llx %d %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
-                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.smem32, kv.second.ms);
+                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.smem_fill, kv.second.ms);
     std::fclose(fp);
     return BOLT_OK;
 }
@@ -1775,10 +1744,10 @@ extern "C" bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path) {
     unsigned long long key;
     bolt_ctx::GbTune t{};
     while (std::fscanf(fp, "%llx %d %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift,
-                       &t.smem32, &t.ms) == 7) {
+                       &t.smem_fill, &t.ms) == 7) {
         const bool valid = (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
                            t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 1 &&
-                           t.load_shift <= 3 && (t.smem32 == 0 || t.smem32 == 1);
+                           t.load_shift <= 3 && t.smem_fill >= 1 && t.smem_fill <= 8;
         if (valid) ctx->tune[(uint64_t)key] = t;
     }
     std::fclose(fp);

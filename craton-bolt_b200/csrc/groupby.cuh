@@ -76,8 +76,10 @@ struct alignas(16) GbParams {
     int32_t smem_log2;   // 0 disables the shared-memory tier
     int32_t fx_e;
     int32_t warp_agg;
-    int32_t smem32;      // shared tier merges with native 32-bit atomics
+    uint32_t smem_fill;  // keys the shared tier admits before it only serves lookups
     int32_t spec;        // compiled row-loop layout (gb_spec_of), 0 = generic
+    int32_t cnt32;       // COUNT fits 32 bits per shared table (see merge_words_smem)
+    int32_t pad1;
     uint32_t* status;
     ull* occupancy;
     ull grow_limit;
@@ -131,7 +133,7 @@ struct GbPlan {
     uint32_t flags = 0;
     ull* words = nullptr;  // device: [0] occupancy, [1] non-NULL groups, [2] groups, [3] status
     uint64_t shape = 0;    // autotuning key of the query shape
-    bolt_ctx::GbTune tune{512, 0, 1, 1, 1, 0.0};
+    bolt_ctx::GbTune tune{512, 1, 0, 2, 4, 0.0};
 };
 
 // Key of a query shape for the autotuning cache: key / predicate / state
