@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 namespace bolt {
 namespace {
@@ -1561,6 +1562,158 @@ extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc
     if (desc->n_keys >= 1 && desc->key_cols && desc->cols && desc->key_cols[0] >= 0 && desc->key_cols[0] < desc->n_cols)
         nrows = desc->cols[desc->key_cols[0]].len;
     return gb_single(ctx, desc, out, 0, nrows, flags, (cudaStream_t)stream, nullptr, nullptr, "GROUP BY");
+}
+
+// ---------------------------------------------------------------------------
+// GROUP BY that allocates nothing (bolt_groupby_noalloc)
+// ---------------------------------------------------------------------------
+// Some callers may not allocate device memory at all: an engine whose own
+// pool allocator owns every byte of HBM (a stray cudaMalloc there fails or
+// fragments the pool), or a latency-critical loop in which cudaMalloc /
+// cudaFree would synchronise the whole device. They cannot create a
+// bolt_ctx, whose scratch arena is one cudaMalloc. bolt_groupby_noalloc
+// serves them for small group counts: the hash table, the group counters and
+// the finalize descriptor live in the fixed array below, which every GPU that
+// loads this library holds until the process exits.
+//
+// In host code the array's name is only a stand-in for it, so the device
+// address is resolved with cudaGetSymbolAddress: on the first call on each
+// device, with that device current. Make that first call before any stream
+// capture. Every call reuses the same array and clears the part that must
+// start at zero, so calls that overlap on the GPU (different streams or
+// host threads) race on it and corrupt each other: serialise them.
+constexpr uint64_t NOALLOC_SCRATCH_BYTES = 2ull << 20;  // 2 MiB
+constexpr uint64_t NOALLOC_MAX_SLOTS = 8192;            // table slots -> at most 6144 groups
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_noalloc_scratch on `dev`, which must be current.
+bool noalloc_scratch(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return false;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return false;
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return true;
+}
+
+}  // namespace
+
+extern "C" bolt_status bolt_groupby_noalloc(const bolt_groupby_desc* desc, bolt_groupby_out* out,
+                                            bolt_stream stream, char* err, int32_t err_cap) {
+    auto report = [&](bolt_status st, const char* msg) {
+        if (err && err_cap > 0) std::snprintf(err, (size_t)err_cap, "%s", msg);
+        return st;
+    };
+    if (!desc || !out) return report(BOLT_ERR_INVALID, "bolt_groupby_noalloc: null descriptor or output");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: no current device");
+    unsigned char* base = nullptr;
+    if (!noalloc_scratch(dev, &base))
+        return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: cudaGetSymbolAddress of the static scratch failed");
+    cudaStream_t s = (cudaStream_t)stream;
+
+    // A host-only context: device attributes for the planner and a place for
+    // its error text; it owns no device memory.
+    bolt_ctx c;
+    c.device = dev;
+    if (cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: device attribute query failed");
+    // Scratch layout: [0, 256) status word and counters, then the finalize
+    // descriptor, then the hash table.
+    ull* words = reinterpret_cast<ull*>(base);
+    GbFinal* d_final = reinterpret_cast<GbFinal*>(base + 256);
+    ull* table = reinterpret_cast<ull*>(base + 256 + ((sizeof(GbFinal) + 255) & ~size_t(255)));
+    const uint64_t table_room = NOALLOC_SCRATCH_BYTES - (uint64_t)(reinterpret_cast<unsigned char*>(table) - base);
+
+    uint64_t nrows = 0;
+    if (desc->n_keys >= 1 && desc->key_cols && desc->cols && desc->key_cols[0] >= 0 && desc->key_cols[0] < desc->n_cols)
+        nrows = desc->cols[desc->key_cols[0]].len;
+    const uint64_t want =
+        desc->groups_hint ? 1ull << ceil_log2_u64(2 * desc->groups_hint + 16) : NOALLOC_MAX_SLOTS;
+    const uint64_t cap = std::max<uint64_t>(64, std::min<uint64_t>(want, NOALLOC_MAX_SLOTS));
+    int mode = 0;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        GbPlan pl;
+        bolt_status st = gb_plan(&c, desc, out, 0, nrows, BOLT_FLAG_NO_TUNE, mode, cap, &pl);
+        if (st != BOLT_OK) return report(st, c.last_error.c_str());
+        const uint64_t table_bytes = (pl.cap + 2) * (uint64_t)pl.prm.slot_words * 8;
+        if (table_bytes > table_room)
+            return report(BOLT_ERR_CAPACITY,
+                          "bolt_groupby_noalloc: the hash table for this aggregate list exceeds the 2 MiB static scratch");
+        GbParams& p = pl.prm;
+        GbFinal& f = pl.fin;
+        p.gtab = table;
+        p.status = reinterpret_cast<uint32_t*>(words);
+        p.occupancy = words + 1;
+        p.i64_bits = nullptr;
+        for (int s2 = 0; s2 < p.n_st; ++s2)
+            if (p.st[s2].kind == K_SUM_I64) p.i64_bits = reinterpret_cast<uint32_t*>(words + 4);
+        f.gtab = table;
+        f.status = p.status;
+        f.n_nonnull = words + 2;
+        f.n_groups = words + 3;
+        f.n_groups_user = nullptr;
+        // The previous call left its table and counters in the array.
+        if (cudaMemsetAsync(words, 0, 256, s) != cudaSuccess || cudaMemsetAsync(table, 0, table_bytes, s) != cudaSuccess)
+            return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: clearing the static scratch failed");
+        if (cudaMemcpyAsync(d_final, &f, sizeof(GbFinal), cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: descriptor upload failed");
+        const size_t smem = (size_t)pl.smem_entries * 8ull * (size_t)p.slot_words;
+        const uint64_t tile = (uint64_t)pl.block * pl.u;
+        const uint64_t tiles = (p.n_rows + tile - 1) / tile;
+        const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)c.num_sms, std::max<uint64_t>(tiles, 1));
+        if (p.n_rows > 0) {
+            const AggKernel kfn = agg_kernel_for(p.spec, p.n_st);
+            if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: shared-memory attribute failed");
+            kfn<<<grid, pl.block, smem, s>>>(p);
+            if (cudaGetLastError() != cudaSuccess)
+                return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: aggregation launch failed");
+        }
+        const size_t fsm = (size_t)pl.cap * 2 * 12;
+        if (cudaFuncSetAttribute(gb_small_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) !=
+            cudaSuccess)
+            return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: shared-memory attribute failed");
+        gb_small_final_kernel<<<1, 1024, fsm, s>>>(d_final);
+        if (cudaGetLastError() != cudaSuccess) return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: finalize launch failed");
+        ull w[5] = {0, 0, 0, 0, 0};
+        if (cudaMemcpyAsync(w, words, sizeof w, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: kernel or readback failed");
+        const uint32_t fl = (uint32_t)w[0];
+        out->n_groups = w[3];
+        if (fl & (ST_FLAG_GROW | ST_FLAG_SPILL))
+            return report(BOLT_ERR_CAPACITY,
+                          "bolt_groupby_noalloc: more than 6144 groups (8192-slot table limit); use bolt_groupby");
+        if (fl & (ST_FLAG_RANGE | ST_FLAG_DECRANGE)) {
+            if (fl & ST_FLAG_RANGE) mode |= GB_MODE_F64_ATOMIC;
+            if (fl & ST_FLAG_DECRANGE) mode |= GB_MODE_WIDE_DEC;
+            continue;
+        }
+        if (fl & ST_FLAG_DECOVERFLOW)
+            return report(BOLT_ERR_OVERFLOW, "SUM(Decimal128) precision overflow: accumulator exceeds i128 range");
+        if (fl & ST_FLAG_OVERFLOW)
+            return report(BOLT_ERR_OVERFLOW, "SUM(integer) overflow: accumulator exceeds i64 range");
+        if (fl & ST_FLAG_CAPACITY) return report(BOLT_ERR_CAPACITY, "bolt_groupby_noalloc: output capacity exceeded");
+        if (fl) return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: unexpected device status");
+        if (p.i64_bits && (uint32_t)w[4] + (uint32_t)ceil_log2_u64(p.n_rows + 1) >= 63)
+            return report(BOLT_DECLINE, "bolt_groupby_noalloc: SUM(Int64) inputs large enough to need the row-order "
+                                        "overflow check; use bolt_groupby");
+        if (err && err_cap > 0) err[0] = 0;
+        return BOLT_OK;
+    }
+    return report(BOLT_ERR_CAPACITY, "bolt_groupby_noalloc: accumulator mode retries did not converge");
 }
 
 // Fused probe -> GROUP BY <build payload>: the GROUP BY kernel with a join

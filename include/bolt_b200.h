@@ -193,6 +193,22 @@ typedef struct {
 bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc,
                          bolt_groupby_out* out, uint32_t flags, bolt_stream stream);
 
+/* GROUP BY that allocates no device memory. No counterpart in the
+ * reference. For callers that may not call cudaMalloc / cudaFree at all (an
+ * engine whose own pool owns all of HBM, or a latency-critical loop where an
+ * allocation would synchronise the device) and so cannot hold a bolt_ctx.
+ * Same semantics and outputs as bolt_groupby (device columns in, device
+ * columns out), for at most 6144 groups (an 8192-slot table). Its scratch is
+ * one fixed 2 MiB device array inside this library, held by every GPU that
+ * loads it until the process exits. The first call on a device (with that
+ * device current) resolves the array's address: make it before any stream
+ * capture. Calls share the array and clear it on entry, so calls that
+ * overlap on the GPU race: serialise them. The call synchronises `stream`.
+ * More groups -> BOLT_ERR_CAPACITY; `err` (nullable, err_cap bytes) receives
+ * the message of a failure. */
+bolt_status bolt_groupby_noalloc(const bolt_groupby_desc* desc, bolt_groupby_out* out,
+                                 bolt_stream stream, char* err, int32_t err_cap);
+
 /* Autotuner (replaces the reference's fixed dispatch thresholds,
  * groupby_shmem_dispatch.rs:126-131, groupby_tier2_dispatch.rs:171-225):
  * times the GROUP BY of `desc` on the device under candidate launch choices
