@@ -35,6 +35,8 @@ FLAG_PROFILE = 0x2
 FLAG_FORCE_GLOBAL = 0x4
 FLAG_FORCE_SHMEM = 0x8
 FLAG_NO_TUNE = 0x10
+FLAG_KERNEL_REGS = 0x20
+FLAG_KERNEL_STAGED = 0x40
 
 
 class ColView(C.Structure):

@@ -128,29 +128,30 @@ __device__ __forceinline__ double i128_to_double_scaled(ull lo, ll hi, int e) {
     return neg ? -d : d;
 }
 
-// float64 -> round-half-away 128-bit fixed point with e fractional bits.
-// Returns false for non-finite values or |v| >= 2^32 (the window the scale
-// was chosen for).
+// float64 -> 128-bit fixed point with e fractional bits (0 <= e <= 1000),
+// rounded to nearest-even at bit -e. Returns false for non-finite values or
+// |v| >= 2^32 (the window the scale was chosen for).
+//
+// Done in float64 arithmetic, which is exact here: t = |v| * 2^e is a
+// power-of-two scaling; h = floor(t / 2^64) is exact; r = t - h * 2^64 lies in
+// [0, 2^64) and is a multiple of ulp(t), so it has at most 53 significant bits
+// (when t >= 2^64, ulp(t) >= 2^12) and the fused multiply-add yields it
+// exactly. Only the final conversion of r rounds.
 __device__ __forceinline__ bool f64_to_fixed(double v, int e, ull& lo, ll& hi) {
-    ull b = (ull)__double_as_longlong(v);
-    int E = (int)((b >> 52) & 0x7FF);
-    ull m = b & ((1ull << 52) - 1);
-    if (E == 0x7FF) return false;
-    if (E == 0) {
-        if (m == 0) { lo = 0; hi = 0; return true; }
-        E = 1;
-    } else {
-        m |= 1ull << 52;
+    const double a = fabs(v);
+    if (!(a < 4294967296.0)) return false;  // also NaN and infinities
+    const double scale = __longlong_as_double((ll)(1023 + e) << 52);
+    const double t = a * scale;
+    const double h = floor(t * 0x1p-64);
+    const double r = fma(-h, 0x1p64, t);
+    ull l = __double2ull_rn(r);
+    ull u = (ull)__double2ll_rz(h);
+    if (__double_as_longlong(v) < 0) {  // negate the 128-bit magnitude
+        l = ~l + 1ull;
+        u = ~u + (l == 0 ? 1ull : 0ull);
     }
-    if (E - 1023 >= 32) return false;
-    int s = E - 1075 + e;
-    unsigned __int128 mag;
-    if (s >= 0) mag = (unsigned __int128)m << s;
-    else if (s > -63) mag = (unsigned __int128)((m + (1ull << (-s - 1))) >> (-s));
-    else mag = 0;
-    if (b >> 63) mag = (unsigned __int128)0 - mag;
-    lo = (ull)mag;
-    hi = (ll)(ull)(mag >> 64);
+    lo = l;
+    hi = (ll)u;
     return true;
 }
 

@@ -46,7 +46,11 @@ struct bolt_ctx {
     StageUse stage_use[STAGE_SLOTS] = {};
     uint32_t stage_next = 0;
     // Autotuned GROUP BY launch choices per query shape (see gb_shape_key).
-    struct GbTune { int32_t block, smem_shift, warp_agg, load_shift, smem_fill; double ms; };  // smem_fill in eighths
+    // GROUP BY launch choices: block size, shared-table shrink (8 = no shared
+    // tier), warp pre-aggregation, table load (1 << load_shift - 1 headroom),
+    // shared-table admission in eighths, and the staged kernel's 32-row
+    // chunks per consumer warp (0 = the register kernel).
+    struct GbTune { int32_t block, smem_shift, warp_agg, load_shift, smem_fill, staged; double ms; };
     std::unordered_map<uint64_t, GbTune> tune;
 };
 

@@ -30,6 +30,7 @@
 #include "groupby.cuh"
 #include "join.cuh"
 #include "radix_sort.cuh"
+#include "bulk.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -67,28 +68,35 @@ __device__ __forceinline__ ull pack_key(const GbParams& p, uint64_t r) {
     return (hi << 32) | lo;
 }
 
+__device__ __forceinline__ bool cmp_i(ll v, int cmp, ll lit) {
+    switch (cmp) {
+    case BOLT_CMP_LT: return v < lit;
+    case BOLT_CMP_LE: return v <= lit;
+    case BOLT_CMP_GT: return v > lit;
+    case BOLT_CMP_GE: return v >= lit;
+    case BOLT_CMP_EQ: return v == lit;
+    default: return v != lit;
+    }
+}
+
+__device__ __forceinline__ bool cmp_f(double v, int cmp, double lit) {
+    switch (cmp) {
+    case BOLT_CMP_LT: return v < lit;
+    case BOLT_CMP_LE: return v <= lit;
+    case BOLT_CMP_GT: return v > lit;
+    case BOLT_CMP_GE: return v >= lit;
+    case BOLT_CMP_EQ: return v == lit;
+    default: return v != lit;
+    }
+}
+
 __device__ __forceinline__ bool eval_pred(const PredDesc& d, uint64_t r) {
     if (!bit_valid(d.valid, r)) return false;
-    if (d.dtype == BOLT_F64 || d.dtype == BOLT_F32) {
-        double v = d.dtype == BOLT_F64 ? ld_stream((const double*)d.col + r)
-                                       : (double)ld_stream((const float*)d.col + r);
-        switch (d.cmp) {
-        case BOLT_CMP_LT: return v < d.lit_f;
-        case BOLT_CMP_LE: return v <= d.lit_f;
-        case BOLT_CMP_GT: return v > d.lit_f;
-        case BOLT_CMP_GE: return v >= d.lit_f;
-        case BOLT_CMP_EQ: return v == d.lit_f;
-        default: return v != d.lit_f;
-        }
-    }
-    ll v = d.dtype == BOLT_I32 ? (ll)ld_stream((const int32_t*)d.col + r) : ld_stream((const ll*)d.col + r);
-    switch (d.cmp) {
-    case BOLT_CMP_LT: return v < d.lit_i;
-    case BOLT_CMP_LE: return v <= d.lit_i;
-    case BOLT_CMP_GT: return v > d.lit_i;
-    case BOLT_CMP_GE: return v >= d.lit_i;
-    case BOLT_CMP_EQ: return v == d.lit_i;
-    default: return v != d.lit_i;
+    switch (d.dtype) {
+    case BOLT_F64: return cmp_f(ld_stream((const double*)d.col + r), d.cmp, d.lit_f);
+    case BOLT_F32: return cmp_f((double)ld_stream((const float*)d.col + r), d.cmp, d.lit_f);
+    case BOLT_I64: return cmp_i(ld_stream((const ll*)d.col + r), d.cmp, d.lit_i);
+    default: return cmp_i((ll)ld_stream((const int32_t*)d.col + r), d.cmp, d.lit_i);
     }
 }
 
@@ -330,14 +338,101 @@ __device__ __forceinline__ int snum(const GbParams& p) {
     else return SP::n;
 }
 
+// Folds one row (already loaded and filtered: row_in) into the shared or
+// global table. Every lane of the warp calls it together (the warp-level
+// pre-aggregation is collective); lanes without a row pass row_in = false.
+template <int MAXS, class SP>
+__device__ __forceinline__ void row_fold(const GbParams& p, ull* sk, ull* sw, int C, uint32_t* fill, bool row_in,
+                                         bool knull, ull stored, const ull (&raw)[MAXS], uint32_t vbits,
+                                         uint32_t dfit, uint64_t r, uint32_t& inserts, uint32_t& absbits) {
+    const int SW = p.slot_words - 1;
+    const uint32_t lane = lane_id();
+    const int NS = snum<SP>(p);
+    bool row = row_in;
+    ull c0[MAXS], c1[MAXS];
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+        c0[s] = 0;
+        c1[s] = 0;
+        if (row && s < NS)
+            contribution(p, p.st[s], skind<SP>(p, s), raw[s], (vbits >> s) & 1, (dfit >> s) & 1,
+                         r, c0[s], c1[s]);
+    }
+    // Bit length of the largest |v| fed to an int64 SUM: decides whether
+    // a row-order prefix of some group could leave the i64 range (then
+    // the exact row-order check runs after the query).
+    if (row && p.i64_bits) {
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+            if (s < NS && skind<SP>(p, s) == K_SUM_I64 && ((vbits >> s) & 1)) {
+                const ll v = (ll)raw[s];
+                const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
+                const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
+                absbits = b > absbits ? b : absbits;
+            }
+        }
+    }
+    // Special groups: the NULL key and the key whose complement is 0.
+    const bool special = row && (knull || stored == 0);
+    if (special) {
+        const ull slot = (1ull << p.log2cap) + (knull ? 1 : 0);
+        ull* w = p.gtab + slot * (ull)p.slot_words;
+        if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s)
+            if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+        row = false;
+    }
+    // Warp-level pre-aggregation of duplicate keys.
+    if (p.warp_agg) {
+        const uint32_t act = __ballot_sync(0xffffffffu, row);
+        uint32_t peers = 0;
+        if (row) peers = __match_any_sync(act, stored);
+        const bool leader = row && (uint32_t)(__ffs(peers) - 1) == lane;
+        uint32_t others = leader ? (peers & ~(1u << lane)) : 0u;
+        const int rounds = __reduce_max_sync(0xffffffffu, (uint32_t)__popc(others));
+        for (int it = 0; it < rounds; ++it) {
+            int src = (int)lane;
+            if (others) {
+                src = __ffs(others) - 1;
+                others &= others - 1;
+            }
+#pragma unroll
+            for (int s = 0; s < MAXS; ++s) {
+                if (s < NS) {
+                    const ull b0 = __shfl_sync(0xffffffffu, c0[s], src);
+                    const ull b1 = __shfl_sync(0xffffffffu, c1[s], src);
+                    if (leader && src != (int)lane) combine(skind<SP>(p, s), c0[s], c1[s], b0, b1);
+                }
+            }
+        }
+        row = leader;
+    }
+    if (!row) return;
+    int sl = -1;
+    if (C) sl = s_find_insert(sk, p.smem_log2, stored, fill, p.smem_fill);
+    if (sl >= 0) {
+        ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s)
+            if (s < NS) merge_words_smem(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s], p.cnt32);
+    } else {
+        const int64_t g = g_find_insert(p, stored, inserts);
+        if (g >= 0) {
+            ull* w = p.gtab + (ull)g * p.slot_words;
+#pragma unroll
+            for (int s = 0; s < MAXS; ++s)
+                if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
+        }
+    }
+}
+
 // One tile of blockDim.x * U rows starting at row `base` of the query:
 // load, filter, key, pre-aggregate and fold into the shared or global table.
 // `sk` / `sw` are the shared table's keys and state words (C slots, C may be 0).
 template <int U, int MAXS, class SP>
 __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull* sw, int C, uint32_t* fill,
                                                 uint64_t base, uint32_t& inserts, uint32_t& absbits) {
-    const int SW = p.slot_words - 1;
-    const uint32_t lane = lane_id();
     const uint64_t n = p.n_rows;
     const int NS = snum<SP>(p);
     bool has[U];
@@ -403,85 +498,8 @@ __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull*
     // slot 0 and the later rows move down one slot after each iteration.
 #pragma unroll 1
     for (int u = 0; u < U; ++u) {
-        do {
-            bool row = has[0];
-            ull c0[MAXS], c1[MAXS];
-#pragma unroll
-            for (int s = 0; s < MAXS; ++s) {
-                c0[s] = 0;
-                c1[s] = 0;
-                if (row && s < NS)
-                    contribution(p, p.st[s], skind<SP>(p, s), raw[0][s], (vbits[0] >> s) & 1, (dfit[0] >> s) & 1,
-                                 p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, c0[s], c1[s]);
-            }
-            // Bit length of the largest |v| fed to an int64 SUM: decides whether
-            // a row-order prefix of some group could leave the i64 range (then
-            // the exact row-order check runs after the query).
-            if (row && p.i64_bits) {
-#pragma unroll
-                for (int s = 0; s < MAXS; ++s) {
-                    if (s < NS && skind<SP>(p, s) == K_SUM_I64 && ((vbits[0] >> s) & 1)) {
-                        const ll v = (ll)raw[0][s];
-                        const ull a = v < 0 ? (ull)(-(v + 1)) + 1ull : (ull)v;
-                        const uint32_t b = a ? 64u - (uint32_t)__clzll((ll)a) : 0u;
-                        absbits = b > absbits ? b : absbits;
-                    }
-                }
-            }
-            // Special groups: the NULL key and the key whose complement is 0.
-            const bool special = row && (knull[0] || stored[0] == 0);
-            if (special) {
-                const ull slot = (1ull << p.log2cap) + (knull[0] ? 1 : 0);
-                ull* w = p.gtab + slot * (ull)p.slot_words;
-                if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
-#pragma unroll
-                for (int s = 0; s < MAXS; ++s)
-                    if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
-                row = false;
-            }
-            // Warp-level pre-aggregation of duplicate keys.
-            if (p.warp_agg) {
-                const uint32_t act = __ballot_sync(0xffffffffu, row);
-                uint32_t peers = 0;
-                if (row) peers = __match_any_sync(act, stored[0]);
-                const bool leader = row && (uint32_t)(__ffs(peers) - 1) == lane;
-                uint32_t others = leader ? (peers & ~(1u << lane)) : 0u;
-                const int rounds = __reduce_max_sync(0xffffffffu, (uint32_t)__popc(others));
-                for (int it = 0; it < rounds; ++it) {
-                    int src = (int)lane;
-                    if (others) {
-                        src = __ffs(others) - 1;
-                        others &= others - 1;
-                    }
-#pragma unroll
-                    for (int s = 0; s < MAXS; ++s) {
-                        if (s < NS) {
-                            const ull b0 = __shfl_sync(0xffffffffu, c0[s], src);
-                            const ull b1 = __shfl_sync(0xffffffffu, c1[s], src);
-                            if (leader && src != (int)lane) combine(skind<SP>(p, s), c0[s], c1[s], b0, b1);
-                        }
-                    }
-                }
-                row = leader;
-            }
-            if (!row) continue;
-            int sl = -1;
-            if (C) sl = s_find_insert(sk, p.smem_log2, stored[0], fill, p.smem_fill);
-            if (sl >= 0) {
-                ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
-#pragma unroll
-                for (int s = 0; s < MAXS; ++s)
-                    if (s < NS) merge_words_smem(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s], p.cnt32);
-            } else {
-                const int64_t g = g_find_insert(p, stored[0], inserts);
-                if (g >= 0) {
-                    ull* w = p.gtab + (ull)g * p.slot_words;
-#pragma unroll
-                    for (int s = 0; s < MAXS; ++s)
-                        if (s < NS) merge_words(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s]);
-                }
-            }
-        } while (0);
+        row_fold<MAXS, SP>(p, sk, sw, C, fill, has[0], knull[0], stored[0], raw[0], vbits[0], dfit[0],
+                           p.row_begin + base + (uint64_t)u * blockDim.x + threadIdx.x, inserts, absbits);
 #pragma unroll
         for (int v = 0; v + 1 < U; ++v) {
             has[v] = has[v + 1];
@@ -569,6 +587,230 @@ __global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_agg_kernel(const 
     for (uint64_t base = (uint64_t)blockIdx.x * tile; base < p.n_rows; base += (uint64_t)gridDim.x * tile) {
         gb_process_tile<U, MAXS, SP>(p, sk, sw, C, &s_fill, base, inserts, absbits);
         if (gb_warp_epilogue(p, inserts, pending)) break;
+    }
+    gb_warp_flush_pending(p, pending);
+    gb_flush_absbits(p, absbits);
+    __syncthreads();
+    gb_flush_shared(p, sk, sw, C);
+}
+
+// ---------------------------------------------------------------------------
+// Staged aggregation kernel.
+//
+// Warp 0 of the CTA is the producer: its lane 0 streams tiles of tile_rows
+// rows of every input column into a ring of n_stages shared-memory stages
+// with bulk copies (cp.async.bulk) that complete on the stage's `full`
+// mbarrier. The other warps are consumers: each takes its `chunks` x 32
+// contiguous rows of the tile, evaluates the WHERE conjuncts, compacts the
+// surviving row numbers into a per-warp list, and folds the survivors 32 to
+// a warp step, so filtered-out rows cost no aggregation work. A consumer
+// releases the stage on its `empty` mbarrier (count: consumer warps).
+//
+// Only whole tiles are staged; the last n_rows % tile_rows rows are folded
+// from global memory after the ring drains. All waits are bounded.
+// ---------------------------------------------------------------------------
+template <bool STAGED>
+__device__ __forceinline__ const unsigned char* sc_base(const GbParams& p, int c, const unsigned char* stage,
+                                                       uint64_t tile_row0) {
+    if (STAGED) return stage + p.sc_off[c];
+    return static_cast<const unsigned char*>(p.sc_col[c]) + (p.row_begin + tile_row0) * (uint64_t)p.sc_w[c];
+}
+
+__device__ __forceinline__ bool pred_at(const GbParams& p, int q, const unsigned char* base, uint32_t i) {
+    const PredDesc& d = p.pred[q];
+    switch (d.dtype) {
+    case BOLT_F64: return cmp_f(reinterpret_cast<const double*>(base)[i], d.cmp, d.lit_f);
+    case BOLT_F32: return cmp_f((double)reinterpret_cast<const float*>(base)[i], d.cmp, d.lit_f);
+    case BOLT_I64: return cmp_i(reinterpret_cast<const ll*>(base)[i], d.cmp, d.lit_i);
+    default: return cmp_i((ll)reinterpret_cast<const int32_t*>(base)[i], d.cmp, d.lit_i);
+    }
+}
+
+__device__ __forceinline__ uint32_t key32_at(int dt, const unsigned char* base, uint32_t i) {
+    if (dt == BOLT_F32) return canon_f32_bits(reinterpret_cast<const float*>(base)[i]);
+    return (uint32_t)reinterpret_cast<const int32_t*>(base)[i];
+}
+
+__device__ __forceinline__ ull key_at(const GbParams& p, const unsigned char* b0, const unsigned char* b1,
+                                      uint32_t i) {
+    if (p.n_keys == 1) {
+        switch (p.kdtype[0]) {
+        case BOLT_I32: return (ull)(ll)reinterpret_cast<const int32_t*>(b0)[i];
+        case BOLT_I64: return (ull)reinterpret_cast<const ll*>(b0)[i];
+        case BOLT_F32: return (ull)canon_f32_bits(reinterpret_cast<const float*>(b0)[i]);
+        default: return canon_f64_bits(reinterpret_cast<const double*>(b0)[i]);
+        }
+    }
+    return ((ull)key32_at(p.kdtype[0], b0, i) << 32) | (ull)key32_at(p.kdtype[1], b1, i);
+}
+
+__device__ __forceinline__ ull raw_at(int dt, const unsigned char* base, uint32_t i, bool& dec_fits) {
+    switch (dt) {
+    case BOLT_I32: return (ull)(ll)reinterpret_cast<const int32_t*>(base)[i];
+    case BOLT_I64: return (ull)reinterpret_cast<const ll*>(base)[i];
+    case BOLT_F32: return (ull)__double_as_longlong((double)reinterpret_cast<const float*>(base)[i]);
+    case BOLT_F64: return (ull)__double_as_longlong(reinterpret_cast<const double*>(base)[i]);
+    default: {  // DEC128
+        const ulonglong2 v = reinterpret_cast<const ulonglong2*>(base)[i];
+        dec_fits = (ll)v.y == ((ll)v.x >> 63);
+        return v.x;
+    }
+    }
+}
+
+// Filters, compacts and folds the rows [first, first + 32 * nchunks) of one
+// tile (tile-relative numbers, below `limit`) for the calling warp. `list` is
+// the warp's compaction buffer of 32 * nchunks entries.
+template <class SP, bool STAGED>
+__device__ __forceinline__ void staged_rows(const GbParams& p, ull* sk, ull* sw, int C, uint32_t* fill,
+                                            const unsigned char* stage, uint64_t tile_row0, uint32_t first,
+                                            int nchunks, uint32_t limit, uint16_t* list, uint32_t& inserts,
+                                            uint32_t& absbits) {
+    constexpr int MAXS = SP::n;
+    const uint32_t lane = lane_id();
+    uint32_t cnt = 0;
+    for (int c = 0; c < nchunks; ++c) {
+        const uint32_t i = first + (uint32_t)c * 32u + lane;
+        const uint64_t r = p.row_begin + tile_row0 + i;
+        bool ok = i < limit;
+        if (ok) {
+            for (int q = 0; q < p.n_pred; ++q)
+                ok = ok && bit_valid(p.pred[q].valid, r) &&
+                     pred_at(p, q, sc_base<STAGED>(p, p.pr_sc[q], stage, tile_row0), i);
+            if (p.n_keys > 1)
+                for (int k = 0; k < p.n_keys; ++k) ok = ok && bit_valid(p.kvalid[k], r);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        if (ok) list[cnt + __popc(m & lanemask_lt())] = (uint16_t)(i - first);
+        cnt += __popc(m);
+    }
+    __syncwarp();
+    const unsigned char* kb0 = sc_base<STAGED>(p, p.k_sc[0], stage, tile_row0);
+    const unsigned char* kb1 = p.n_keys > 1 ? sc_base<STAGED>(p, p.k_sc[1], stage, tile_row0) : kb0;
+    for (uint32_t b = 0; b < cnt; b += 32) {
+        const bool has = b + lane < cnt;
+        const uint32_t i = first + (has ? (uint32_t)list[b + lane] : 0u);
+        const uint64_t r = p.row_begin + tile_row0 + i;
+        ull raw[MAXS];
+        uint32_t vbits = 0, dfit = 0;
+        bool knull = false;
+        ull stored = 0;
+        if (has) {
+            stored = ~key_at(p, kb0, kb1, i);
+            if (p.n_keys == 1) knull = !bit_valid(p.kvalid[0], r);
+        }
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+            raw[s] = 0;
+            if (!has) continue;
+            if (p.st_sc[s] >= 0) {
+                bool fits = true;
+                raw[s] = raw_at(p.st[s].dtype, sc_base<STAGED>(p, p.st_sc[s], stage, tile_row0), i, fits);
+                if (bit_valid(p.st[s].valid, r)) vbits |= 1u << s;
+                if (fits) dfit |= 1u << s;
+            } else {
+                vbits |= 1u << s;  // COUNT(*)
+                dfit |= 1u << s;
+            }
+        }
+        row_fold<MAXS, SP>(p, sk, sw, C, fill, has, knull, stored, raw, vbits, dfit, r, inserts, absbits);
+    }
+    __syncwarp();
+}
+
+template <class SP>
+__global__ void __launch_bounds__(1024, 1) gb_staged_kernel(const __grid_constant__ GbParams p) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ __align__(8) uint64_t full[4], empty[4];
+    __shared__ uint32_t s_fill;
+    const int S = p.n_stages;
+    const int NW = (int)(blockDim.x >> 5) - 1;  // consumer warps
+    const int warp = (int)(threadIdx.x >> 5);
+    const uint32_t lane = lane_id();
+    const int SW = p.slot_words - 1;
+    const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
+    unsigned char* stages = dsm;
+    ull* sk = reinterpret_cast<ull*>(dsm + (size_t)S * p.stage_bytes);
+    ull* sw = sk + C;
+    uint16_t* lists = reinterpret_cast<uint16_t*>(sw + (size_t)C * SW);
+    const uint32_t T = p.tile_rows;
+    const uint64_t ntiles = p.n_rows / T;
+
+    for (int i = threadIdx.x; i < C * (SW + 1); i += blockDim.x) sk[i] = 0;
+    if (threadIdx.x == 0) {
+        s_fill = 0;
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], (uint32_t)NW);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    uint32_t inserts = 0, pending = 0, absbits = 0;
+    if (warp == 0) {
+        if (lane == 0) {
+            const uint64_t pol = l2_evict_first_policy();
+            uint32_t j = 0;
+            bool ok = true;
+            for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+                const int st = (int)(j % (uint32_t)S);
+                const uint32_t use = j / (uint32_t)S;
+                if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                const bool stop = (*reinterpret_cast<volatile uint32_t*>(p.status) &
+                                   (ST_FLAG_GROW | ST_FLAG_SPILL | ST_FLAG_TIMEOUT)) != 0;
+                if (stop) {
+                    mbar_arrive(&full[st]);  // completes the phase with no data
+                } else {
+                    mbar_arrive_expect_tx(&full[st], p.stage_bytes);
+                    unsigned char* dst = stages + (size_t)st * p.stage_bytes;
+                    for (int c = 0; c < p.n_sc; ++c) {
+                        const uint32_t w = (uint32_t)p.sc_w[c];
+                        const unsigned char* src =
+                            static_cast<const unsigned char*>(p.sc_col[c]) + (p.row_begin + t * T) * (uint64_t)w;
+                        bulk_load(dst + p.sc_off[c], src, T * w, &full[st], pol);
+                    }
+                }
+            }
+            // The copies of the last (up to S) tiles may still be landing if a
+            // consumer gave up early: wait for them before the CTA can exit.
+            const uint32_t issued = j;
+            for (uint32_t k = issued > (uint32_t)S ? issued - (uint32_t)S : 0u; k < issued; ++k)
+                if (!mbar_wait(&full[k % (uint32_t)S], (k / (uint32_t)S) & 1u)) ok = false;
+            if (!ok) atomicOr(p.status, ST_FLAG_TIMEOUT);
+        }
+        __syncwarp();
+    } else {
+        const int cw = warp - 1;
+        uint16_t* list = lists + (size_t)cw * 32 * p.chunks;
+        uint32_t j = 0;
+        for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+            const int st = (int)(j % (uint32_t)S);
+            const bool ready = mbar_wait(&full[st], (j / (uint32_t)S) & 1u);
+            if (!__all_sync(0xffffffffu, ready)) {
+                if (lane == 0) atomicOr(p.status, ST_FLAG_TIMEOUT);
+                break;
+            }
+            uint32_t stop = 0;
+            if (lane == 0)
+                stop = (*reinterpret_cast<volatile uint32_t*>(p.status) &
+                        (ST_FLAG_GROW | ST_FLAG_SPILL | ST_FLAG_TIMEOUT)) != 0;
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (!stop)
+                staged_rows<SP, true>(p, sk, sw, C, &s_fill, stages + (size_t)st * p.stage_bytes, t * T,
+                                      (uint32_t)cw * 32u * (uint32_t)p.chunks, p.chunks, T, list, inserts, absbits);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);
+            gb_warp_epilogue(p, inserts, pending);
+        }
+        // Rows after the last whole tile, 32 per consumer warp, from global memory.
+        const uint64_t rem0 = ntiles * T;
+        const uint32_t rem = (uint32_t)(p.n_rows - rem0);
+        for (uint32_t c = (uint32_t)(blockIdx.x * NW + cw) * 32u; c < rem; c += gridDim.x * (uint32_t)NW * 32u)
+            staged_rows<SP, false>(p, sk, sw, C, &s_fill, nullptr, rem0, c, 1, rem, list, inserts, absbits);
     }
     gb_warp_flush_pending(p, pending);
     gb_flush_absbits(p, absbits);
@@ -985,6 +1227,18 @@ BatchKernel batch_kernel_for(int spec, int max_st) {
     }
 }
 
+AggKernel staged_kernel_for(int spec) {
+    switch (spec) {
+    case 1: return gb_staged_kernel<Spec1>;
+    case 2: return gb_staged_kernel<Spec2>;
+    case 3: return gb_staged_kernel<Spec3>;
+    case 4: return gb_staged_kernel<Spec4>;
+    case 5: return gb_staged_kernel<Spec5>;
+    case 6: return gb_staged_kernel<Spec6>;
+    default: return gb_staged_kernel<Spec7>;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1196,6 +1450,20 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         p.spec = gb_spec_of(p.st, n_st);
     }
     p.n_st = n_st;
+    // Staged kernel column map: each distinct input column once.
+    p.n_sc = 0;
+    auto sc_of = [&](const void* colp, int dt) -> int8_t {
+        if (!colp) return -1;
+        const int w = dtype_width(dt);
+        for (int c = 0; c < p.n_sc; ++c)
+            if (p.sc_col[c] == colp && p.sc_w[c] == w) return (int8_t)c;
+        p.sc_col[p.n_sc] = colp;
+        p.sc_w[p.n_sc] = w;
+        return (int8_t)p.n_sc++;
+    };
+    for (int k = 0; k < 2; ++k) p.k_sc[k] = k < p.n_keys ? sc_of(p.kcol[k], p.kdtype[k]) : -1;
+    for (int q = 0; q < GB_MAX_PREDS; ++q) p.pr_sc[q] = q < p.n_pred ? sc_of(p.pred[q].col, p.pred[q].dtype) : -1;
+    for (int s2 = 0; s2 < GB_MAX_STATES; ++s2) p.st_sc[s2] = s2 < n_st ? sc_of(p.st[s2].col, p.st[s2].dtype) : -1;
     p.slot_words = word;
     f.slot_words = word;
     f.n_aggs = d->n_aggs;
@@ -1209,12 +1477,14 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
 
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
     pl->shape = gb_shape_key(p, n, d->groups_hint);
-    bolt_ctx::GbTune tn{512, 1, 0, 2, 4, 0.0};
+    bolt_ctx::GbTune tn{512, 1, 0, 2, 4, 0, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
     }
     if (force_tune) tn = *force_tune;
+    if (flags & BOLT_FLAG_KERNEL_REGS) tn.staged = 0;
+    if ((flags & BOLT_FLAG_KERNEL_STAGED) && tn.staged == 0) tn.staged = 2;
     pl->tune = tn;
 
     // Table sizing: (2 << load_shift - 1)x the expected groups (default 2x,
@@ -1286,6 +1556,40 @@ bolt_status launch_batch_agg(bolt_ctx* ctx, cudaStream_t s, BatchKernel kfn, con
 
 }  // namespace
 
+// Whether the staged kernel serves this plan, and its launch shape: one
+// producer warp plus 31 (chunks <= 2) or 15 consumer warps, tiles of
+// consumers x 32 x chunks rows, as many stages (2..4) as fit beside the
+// shared table (which shrinks when two stages do not fit).
+bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& pl, GbStagedLaunch* out) {
+    const GbParams& p = pl.prm;
+    const int chunks = pl.tune.staged;
+    if (chunks <= 0 || p.spec == 0 || p.jslots || p.n_sc == 0) return false;
+    const int block = chunks <= 2 ? 1024 : 512;
+    const int nw = block / 32 - 1;
+    const uint32_t T = (uint32_t)(nw * 32 * chunks);
+    if (p.n_rows < (uint64_t)T) return false;
+    uint64_t row_w = 0;
+    for (int c = 0; c < p.n_sc; ++c) {
+        // Bulk copies need 16-byte aligned tile starts.
+        if (((uintptr_t)p.sc_col[c] + p.row_begin * (uint64_t)p.sc_w[c]) % 16 != 0) return false;
+        row_w += (uint64_t)p.sc_w[c];
+    }
+    const size_t stage = (size_t)T * row_w;
+    const size_t lists = (size_t)nw * 32 * chunks * 2;
+    const size_t budget = (size_t)std::max(ctx->max_smem_optin - 1024, 0);
+    int sl = p.smem_log2;
+    for (;;) {
+        const size_t table = sl ? ((size_t)1 << sl) * 8 * (size_t)p.slot_words : 0;
+        if (table + lists + 2 * stage <= budget) {
+            const int S = (int)std::min<size_t>(4, (budget - table - lists) / stage);
+            if (out) *out = GbStagedLaunch{block, T, S, (uint32_t)stage, sl, (size_t)S * stage + table + lists};
+            return true;
+        }
+        if (sl == 0) return false;
+        sl = sl > 7 ? sl - 1 : 0;
+    }
+}
+
 bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
     if (nq <= 0) return BOLT_OK;
     // Tables and per-query words (occupancy, groups, status) in one zeroed region.
@@ -1325,20 +1629,43 @@ bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t
     if (nq == 1) {
         GbPlan* pl = pls[0];
         GbParams& p = pl->prm;
-        const size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
+        size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
         const uint64_t tile = (uint64_t)pl->block * pl->u;
-        const uint64_t tiles = (p.n_rows + tile - 1) / tile;
-        const AggKernel kfn = agg_kernel_for(p.spec, p.n_st);
+        GbStagedLaunch stg;
+        const bool staged = gb_staged_layout(ctx, *pl, &stg);
+        AggKernel kfn;
+        int block = pl->block;
+        uint64_t tiles;
+        if (staged) {
+            kfn = staged_kernel_for(p.spec);
+            block = stg.block;
+            smem = stg.smem;
+            p.smem_log2 = stg.smem_log2;
+            p.smem_fill = stg.smem_log2 ? (uint32_t)(((1ull << stg.smem_log2) * (uint64_t)pl->tune.smem_fill) / 8) : 0;
+            p.tile_rows = stg.tile_rows;
+            p.n_stages = stg.n_stages;
+            p.stage_bytes = stg.stage_bytes;
+            p.chunks = pl->tune.staged;
+            uint32_t off = 0;
+            for (int c = 0; c < p.n_sc; ++c) {
+                p.sc_off[c] = off;
+                off += stg.tile_rows * (uint32_t)p.sc_w[c];
+            }
+            tiles = std::max<uint64_t>(p.n_rows / stg.tile_rows, 1);
+        } else {
+            kfn = agg_kernel_for(p.spec, p.n_st);
+            tiles = (p.n_rows + tile - 1) / tile;
+        }
         int per_sm = 1;
         BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, pl->block, smem) != cudaSuccess || per_sm < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
             per_sm = 1;
         uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
         if (pl->grid > 0) grid = std::min<uint64_t>(grid, (uint64_t)pl->grid);
         pl->grid = (int)grid;
         if (p.n_rows > 0) {
             kernel_mark_begin(ctx, flags, s);
-            kfn<<<pl->grid, pl->block, smem, s>>>(p);
+            kfn<<<pl->grid, block, smem, s>>>(p);
             ctx->last_launches++;
             kernel_mark_end(ctx, flags, s);
         }
@@ -1834,9 +2161,13 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
                 for (int load_shift : {1, 2})
                     for (int smem_fill : {4, 6}) {
                         if (smem_shift == 8 && smem_fill != 4) continue;  // no shared tier: the fill is moot
-                        cands.push_back({block, smem_shift, warp_agg, load_shift, smem_fill, 0.0});
+                        cands.push_back({block, smem_shift, warp_agg, load_shift, smem_fill, 0, 0.0});
                     }
-    bolt_ctx::GbTune best{512, 1, 0, 2, 4, 1e30};
+    for (int staged : {1, 2, 4})
+        for (int smem_shift : {0, 1})
+            for (int warp_agg : {0, 1})
+                for (int load_shift : {1, 2}) cands.push_back({512, smem_shift, warp_agg, load_shift, 4, staged, 0.0});
+    bolt_ctx::GbTune best{512, 1, 0, 2, 4, 0, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
     for (auto& c : cands) {
@@ -1849,6 +2180,10 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             st = gb_plan(ctx, desc, out, 0, nrows, 0, 0, 0, &pl, &c);
             if (st != BOLT_OK) return st;
             shape = pl.shape;
+            if (c.staged && !gb_staged_layout(ctx, pl, nullptr)) {
+                ok = false;  // the staged kernel does not apply to this query
+                break;
+            }
             BOLT_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
             GbPlan* one = &pl;
             st = gb_run(ctx, &one, 1, s, 0);
@@ -1866,8 +2201,11 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             if (rep > 0) tot += ms;  // first repetition warms up
         }
         if (verbose)
-            std::fprintf(stderr, "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem_fill=%d/8 -> %s%.4f ms\n",
-                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem_fill, ok ? "" : "(flagged) ", tot / 2);
+            std::fprintf(stderr,
+                         "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem_fill=%d/8 staged=%d -> "
+                         "%s%.4f ms\n",
+                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem_fill, c.staged,
+                         ok ? "" : "(not eligible) ", tot / 2);
         if (ok && tot / 2 < best.ms) {
             best = c;
             best.ms = tot / 2;
@@ -1884,8 +2222,9 @@ extern "C" bolt_status bolt_ctx_tuning_save(const bolt_ctx* ctx, const char* pat
     FILE* fp = std::fopen(path, "w");
     if (!fp) return BOLT_ERR_INVALID;
     for (const auto& kv : ctx->tune)
-        std::fprintf(fp, "%llx %d %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
-                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.smem_fill, kv.second.ms);
+        std::fprintf(fp, "%llx %d %d %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
+                     kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.smem_fill,
+                     kv.second.staged, kv.second.ms);
     std::fclose(fp);
     return BOLT_OK;
 }
@@ -1896,11 +2235,12 @@ extern "C" bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path) {
     if (!fp) return fail(ctx, BOLT_ERR_INVALID, "tuning file %s not readable", path);
     unsigned long long key;
     bolt_ctx::GbTune t{};
-    while (std::fscanf(fp, "%llx %d %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift,
-                       &t.smem_fill, &t.ms) == 7) {
+    while (std::fscanf(fp, "%llx %d %d %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift,
+                       &t.smem_fill, &t.staged, &t.ms) == 8) {
         const bool valid = (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
                            t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 1 &&
-                           t.load_shift <= 3 && t.smem_fill >= 1 && t.smem_fill <= 8;
+                           t.load_shift <= 3 && t.smem_fill >= 1 && t.smem_fill <= 8 &&
+                           (t.staged == 0 || t.staged == 1 || t.staged == 2 || t.staged == 4);
         if (valid) ctx->tune[(uint64_t)key] = t;
     }
     std::fclose(fp);

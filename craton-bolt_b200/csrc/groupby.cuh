@@ -24,6 +24,7 @@ enum StKind : int32_t {
 constexpr int GB_MAX_STATES = 8;
 constexpr int GB_MAX_PREDS = 4;
 constexpr int GB_MAX_AGGS = 16;
+constexpr int GB_MAX_SC = 2 + GB_MAX_PREDS + GB_MAX_STATES;  // staged columns
 
 struct StateDesc {
     const void* col;
@@ -94,6 +95,21 @@ struct alignas(16) GbParams {
     int32_t jkdt;
     const void* jkey;
     const uint8_t* jkvalid;
+    // Staged kernel: the distinct input columns (element width, byte offset
+    // inside one stage) and the staged column each key / predicate / state
+    // reads (-1: none).
+    int32_t n_sc;
+    uint32_t stage_bytes;   // one stage: tile_rows x the staged row width
+    uint32_t tile_rows;
+    int32_t n_stages;
+    int32_t chunks;         // 32-row chunks per consumer warp per tile
+    int32_t pad2;
+    const void* sc_col[GB_MAX_SC];
+    int32_t sc_w[GB_MAX_SC];
+    uint32_t sc_off[GB_MAX_SC];
+    int8_t k_sc[2];
+    int8_t pr_sc[GB_MAX_PREDS];
+    int8_t st_sc[GB_MAX_STATES];
 };
 
 struct alignas(16) GbFinal {
@@ -133,7 +149,7 @@ struct GbPlan {
     uint32_t flags = 0;
     ull* words = nullptr;  // device: [0] occupancy, [1] non-NULL groups, [2] groups, [3] status
     uint64_t shape = 0;    // autotuning key of the query shape
-    bolt_ctx::GbTune tune{512, 1, 0, 2, 4, 0.0};
+    bolt_ctx::GbTune tune{512, 1, 0, 2, 4, 0, 0.0};
 };
 
 // Key of a query shape for the autotuning cache: key / predicate / state
@@ -154,6 +170,17 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* desc, const bolt_gro
 
 // Bytes of scratch the plan needs (table + finalize buffers).
 uint64_t gb_plan_scratch(const GbPlan& plan);
+
+// Launch shape of the staged aggregation kernel for one plan.
+struct GbStagedLaunch {
+    int block;
+    uint32_t tile_rows;
+    int n_stages;
+    uint32_t stage_bytes;
+    int smem_log2;
+    size_t smem;
+};
+bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& plan, GbStagedLaunch* out);
 
 // Allocates scratch and enqueues table init, aggregation and finalize of
 // `nq` planned queries (one persistent aggregation launch when nq > 1).

@@ -94,6 +94,75 @@ def test_groupby_filtered_two_key(bolt, engine, oracle, n, n_pairs, hint):
     assert res.n_groups > 1000
 
 
+KERNELS = ["regs", "staged"]
+
+
+def kernel_flags(bolt, kernel):
+    return bolt.FLAG_KERNEL_STAGED if kernel == "staged" else bolt.FLAG_KERNEL_REGS
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_groupby_filtered_two_key_kernels(bolt, engine, oracle, kernel):
+    """Both aggregation kernels on the filtered two-key shape; the row count is
+    not a multiple of any tile, so the staged kernel also folds a remainder."""
+    cols = filtered_config(2_000_077, 1_000_000, seed=17)
+    res, _ = run_both(bolt, engine, oracle, cols, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
+                      hint=400_000, flags=kernel_flags(bolt, kernel))
+    assert res.n_groups > 1000
+
+
+def test_groupby_staged_matches_register_kernel_bitwise(bolt, engine, oracle):
+    cols = filtered_config(1_000_003, 50_000, seed=21)
+    dev, _ = tables(bolt, oracle, cols)
+    r1 = engine.execute_groupby(dev, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
+                                flags=bolt.FLAG_KERNEL_REGS)
+    r2 = engine.execute_groupby(dev, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)],
+                                flags=bolt.FLAG_KERNEL_STAGED)
+    assert r1.n_groups == r2.n_groups
+    for x, y in zip(r1.keys + r1.aggs, r2.keys + r2.aggs):
+        xd = x.data.view(torch.int64) if x.dtype == "f64" else x.data
+        yd = y.data.view(torch.int64) if y.dtype == "f64" else y.data
+        assert torch.equal(xd, yd)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("layout", ["count_sum_i64", "count", "count_sum_i32", "count_sum_f64"])
+def test_groupby_compiled_layouts(bolt, engine, oracle, kernel, layout):
+    """Each compiled state layout, with NULL single keys, f32 / i32 keys and
+    WHERE conjuncts over i32, i64 and f64 columns."""
+    rng = np.random.default_rng(23)
+    n = 700_001
+    k = rng.integers(-3000, 3000, n).astype(np.int32)
+    kv = rng.random(n) > 0.01
+    kf = (rng.integers(-400, 400, n) / 8.0).astype(np.float32)
+    x = rng.normal(0, 1, n)
+    y = rng.integers(-2**40, 2**40, n).astype(np.int64)
+    z = rng.integers(-2**30, 2**30, n).astype(np.int32)
+    f = rng.integers(0, 100, n).astype(np.int32)
+    cols = {"k": (k, bitmap(kv), "i32", 0), "kf": (kf, None, "f32", 0), "x": (x, None, "f64", 0),
+            "y": (y, None, "i64", 0), "z": (z, None, "i32", 0), "f": (f, None, "i32", 0)}
+    where = [("f", "<", 70), ("x", ">", -1.5), ("y", "!=", 12345)]
+    aggs = {"count_sum_i64": [("sum", "y"), ("count_star", None)],
+            "count": [("count_star", None)],
+            "count_sum_i32": [("count_star", None), ("sum", "z")],
+            "count_sum_f64": [("avg", "x")]}[layout]
+    flags = kernel_flags(bolt, kernel)
+    run_both(bolt, engine, oracle, cols, ["k"], aggs, where=where, flags=flags)
+    run_both(bolt, engine, oracle, cols, ["kf"], aggs, where=where[:1], flags=flags)
+
+
+def test_groupby_staged_unaligned_columns_fall_back(bolt, engine, oracle):
+    """Columns that start off a 16-byte boundary take the register kernel."""
+    d = small_config(500_001, seed=29)
+    k = torch.from_numpy(d["k"][0]).to("cuda")
+    v = torch.from_numpy(d["v"][0]).to("cuda")
+    dev = {"k": bolt.Column(k[1:], "i32"), "v": bolt.Column(v[1:], "i64")}
+    host = {"k": oracle.HostCol(d["k"][0][1:].copy(), "i32"), "v": oracle.HostCol(d["v"][0][1:].copy(), "i64")}
+    aggs = [("sum", "v"), ("count_star", None)]
+    res = engine.execute_groupby(dev, ["k"], aggs, groups_hint=1024, flags=bolt.FLAG_KERNEL_STAGED)
+    compare_groupby(res, oracle.groupby(host, ["k"], aggs), ["i32"], aggs, ["i64", None], REL_TOL)
+
+
 def test_groupby_f64_sum_is_order_independent(bolt, engine, oracle):
     """Fixed-point f64 sums: bit-identical across runs and table tiers."""
     cols = filtered_config(500_000, 20_000, seed=7)
