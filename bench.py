@@ -625,13 +625,19 @@ def w_batch(c: Ctx):
     qs = batch_queries(a.batch_queries, n)
     total_rows = sum(q["end"] - q["begin"] for q in qs)
 
-    def prep(q):
+    def prep(q, sliced=False):
+        """A query's descriptor: a row range of the resident columns (batched
+        and served paths), or, for the one-at-a-time bolt_groupby path whose
+        descriptor has no row range, column views of exactly its rows."""
         kname = f"{q['key']}_{q['card']}"
         t = {kname: dev[kname], q["val"]: dev[q["val"]], "f": dev["f"]}
-        return c.eng.prepare_groupby(t, [kname], [("sum", q["val"]), ("count_star", None)], [("f", "<", q["t"])],
-                                     groups_hint=q["card"], rows=(q["begin"], q["end"]))
+        aggs, where = [("sum", q["val"]), ("count_star", None)], [("f", "<", q["t"])]
+        if sliced:
+            t = {k: c.bolt.Column(v.data[q["begin"]:q["end"]], v.dtype) for k, v in t.items()}
+            return c.eng.prepare_groupby(t, [kname], aggs, where, groups_hint=q["card"])
+        return c.eng.prepare_groupby(t, [kname], aggs, where, groups_hint=q["card"], rows=(q["begin"], q["end"]))
 
-    prepared = [prep(q) for q in qs]
+    prepared = [prep(q, sliced=True) for q in qs]
     torch.cuda.synchronize()
     # One at a time: each query through the plain synchronous path.
     t0 = time.perf_counter()

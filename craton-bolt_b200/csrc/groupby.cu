@@ -2071,7 +2071,9 @@ extern "C" bolt_status bolt_join_groupby(bolt_ctx* ctx, const bolt_join_table* t
     d.n_keys = 1;
     d.aggs = aggs;
     d.n_aggs = 2;
-    d.groups_hint = std::min<uint64_t>(std::max<uint64_t>(t->n_build, 1), 2048);
+    // Sized for up to 1024 groups: the table (8192 slots) then finalizes in one
+    // CTA; more groups grow it through the retry.
+    d.groups_hint = std::min<uint64_t>(std::max<uint64_t>(t->n_build, 1), 1024);
     bolt_col_mut agg_out[2] = {*out_sum, *out_count};
     bolt_groupby_out o{};
     o.keys = out_group;
