@@ -267,8 +267,11 @@ class Ctx:
         return ms, launches, kms, sampler.summary(t0, t1)
 
     def time_e2e(self, step, steps: int) -> float:
+        """Device time per call of `step` (host buffers in, host results out),
+        after the warm-up calls that fill the pinned-memory caches."""
         torch = self.torch
-        step()
+        for _ in range(max(self.args.warmup, 3)):
+            step()
         torch.cuda.synchronize()
         self.barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -594,11 +597,11 @@ def w_compact(c: Ctx):
 CARDS = [10, 32, 100, 316, 1000, 3162, 10_000, 31_623, 100_000, 316_228, 1_000_000]
 
 
-def batch_queries(n_q: int, table_rows: int, seed: int = 7):
+def batch_queries(n_q: int, table_rows: int, seed: int = 7, max_rows: float = 5e7):
     rng = np.random.default_rng(seed)
     qs = []
     for i in range(n_q):
-        rows = int(math.exp(rng.uniform(math.log(1e4), math.log(min(5e7, table_rows)))))
+        rows = int(math.exp(rng.uniform(math.log(1e4), math.log(min(max_rows, table_rows)))))
         begin = int(rng.integers(0, table_rows - rows + 1))
         card = CARDS[int(rng.integers(0, len(CARDS)))]
         qs.append({"begin": begin, "end": begin + rows, "card": card, "key": "k32" if i % 2 == 0 else "k64",
@@ -622,8 +625,6 @@ def w_batch(c: Ctx):
         kk = base["k32"] % card
         dev[f"k32_{card}"] = c.bolt.Column(torch.from_numpy(kk.astype(np.int32)).to(c.dev), "i32")
         dev[f"k64_{card}"] = c.bolt.Column(torch.from_numpy(kk * 1_000_003 - (1 << 40)).to(c.dev), "i64")
-    qs = batch_queries(a.batch_queries, n)
-    total_rows = sum(q["end"] - q["begin"] for q in qs)
 
     def prep(q, sliced=False):
         """A query's descriptor: a row range of the resident columns (batched
@@ -637,65 +638,78 @@ def w_batch(c: Ctx):
             return c.eng.prepare_groupby(t, [kname], aggs, where, groups_hint=q["card"])
         return c.eng.prepare_groupby(t, [kname], aggs, where, groups_hint=q["card"], rows=(q["begin"], q["end"]))
 
-    prepared = [prep(q, sliced=True) for q in qs]
-    torch.cuda.synchronize()
-    # One at a time: each query through the plain synchronous path.
-    t0 = time.perf_counter()
-    lat_single = []
-    for pq in prepared:
-        s0 = time.perf_counter()
-        st = c.lib.bolt_groupby(c.eng._ctx, C.byref(pq.desc), C.byref(pq.out), 0, C.c_void_p(c.stream.cuda_stream))
-        if st != 0:
-            raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
-        lat_single.append((time.perf_counter() - s0) * 1e6)
-    single_s = time.perf_counter() - t0
-    single_groups = [int(pq.out.n_groups) for pq in prepared]
-    single_qps = len(qs) / single_s
-    # Served: continuous batching with all queries submitted at once (throughput).
-    scratch = min(a.server_scratch_gb << 30, int(torch.cuda.mem_get_info()[0] * 0.8))
-    srv = c.bolt.Server(c.local, scratch_bytes=scratch, max_batch=a.max_batch, n_lanes=a.lanes)
-    try:
-        prepared2 = [prep(q) for q in qs]
+    def measure(qs):
+        """One-at-a-time bolt_groupby launches vs the continuous-batching
+        server on the same queries: throughput, equality, Poisson latency."""
+        total_rows = sum(q["end"] - q["begin"] for q in qs)
+        prepared = [prep(q, sliced=True) for q in qs]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        tickets = [srv.submit(pq) for pq in prepared2]
-        lat_batch = [srv.wait(t)[1] for t in tickets]
-        batch_s = time.perf_counter() - t0
-        batch_qps = len(qs) / batch_s
-        same = all(int(p2.out.n_groups) == g for p2, g in zip(prepared2, single_groups))
-        # Poisson arrivals at 80% of the one-at-a-time capacity: p50 / p99.
-        rate = 0.8 * single_qps
-        rng = np.random.default_rng(11)
-        gaps = rng.exponential(1.0 / rate, len(qs))
-        prepared3 = [prep(q) for q in qs]
-        torch.cuda.synchronize()
-        tickets = []
-        t0 = time.perf_counter()
-        nxt = t0
-        for pq, gap in zip(prepared3, gaps):
-            nxt += gap
-            while time.perf_counter() < nxt:
-                pass
-            tickets.append(srv.submit(pq))
-        lat_poisson = [srv.wait(t)[1] for t in tickets]
-    finally:
-        srv.close()
+        lat_single = []
+        for pq in prepared:
+            s0 = time.perf_counter()
+            st = c.lib.bolt_groupby(c.eng._ctx, C.byref(pq.desc), C.byref(pq.out), 0,
+                                    C.c_void_p(c.stream.cuda_stream))
+            if st != 0:
+                raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+            lat_single.append((time.perf_counter() - s0) * 1e6)
+        single_s = time.perf_counter() - t0
+        single_groups = [int(pq.out.n_groups) for pq in prepared]
+        single_qps = len(qs) / single_s
+        del prepared
+        scratch = min(a.server_scratch_gb << 30, int(torch.cuda.mem_get_info()[0] * 0.8))
+        srv = c.bolt.Server(c.local, scratch_bytes=scratch, max_batch=a.max_batch, n_lanes=a.lanes)
+        try:
+            prepared2 = [prep(q) for q in qs]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tickets = [srv.submit(pq) for pq in prepared2]
+            for t in tickets:
+                srv.wait(t)
+            batch_s = time.perf_counter() - t0
+            batch_qps = len(qs) / batch_s
+            same = all(int(p2.out.n_groups) == g for p2, g in zip(prepared2, single_groups))
+            del prepared2
+            # Poisson arrivals at 80% of the one-at-a-time capacity: p50 / p99.
+            rate = 0.8 * single_qps
+            rng = np.random.default_rng(11)
+            gaps = rng.exponential(1.0 / rate, len(qs))
+            prepared3 = [prep(q) for q in qs]
+            torch.cuda.synchronize()
+            tickets = []
+            t0 = time.perf_counter()
+            nxt = t0
+            for pq, gap in zip(prepared3, gaps):
+                nxt += gap
+                while time.perf_counter() < nxt:
+                    pass
+                tickets.append(srv.submit(pq))
+            lat_poisson = [srv.wait(t)[1] for t in tickets]
+        finally:
+            srv.close()
+        return {"queries": len(qs), "rows_total": total_rows, "batched_qps": batch_qps,
+                "one_at_a_time_qps": single_qps, "speedup": batch_qps / single_qps,
+                "rows_per_s_batched": total_rows / batch_s, "batch_s": batch_s,
+                "results_equal_alone_vs_mix": same,
+                "latency_us": {"one_at_a_time_p50": float(np.percentile(lat_single, 50)),
+                               "one_at_a_time_p99": float(np.percentile(lat_single, 99)),
+                               "served_poisson_p50": float(np.percentile(lat_poisson, 50)),
+                               "served_poisson_p99": float(np.percentile(lat_poisson, 99)),
+                               "poisson_rate_qps": rate}}
+
+    main_mix = measure(batch_queries(a.batch_queries, n))
+    # The same stream with rows per query log-uniform 10K..1M: launch-bound
+    # queries, where batching is what pays.
+    small_mix = measure(batch_queries(a.batch_queries, n, seed=8, max_rows=1e6))
     line = {
-        "metric": METRIC, "value": batch_qps, "unit": "queries/s", "n_gpus": c.world, "steps": 1,
-        "warmup": 0, "ms_per_step": batch_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": main_mix["batched_qps"], "unit": "queries/s", "n_gpus": c.world, "steps": 1,
+        "warmup": 0, "ms_per_step": main_mix["batch_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32/int64/f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"{len(qs)} filter + GROUP BY queries over resident {n}-row columns, rows/query "
-                               "log-uniform 1e4..5e7, cardinality log-uniform 10..1e6, int32/int64 keys, "
-                               "int64/f64 values", "rows_total": total_rows, "lanes": a.lanes,
-                   "max_batch": a.max_batch},
-        "batched_qps": batch_qps, "one_at_a_time_qps": single_qps, "speedup": batch_qps / single_qps,
-        "rows_per_s_batched": total_rows / batch_s,
-        "results_equal_alone_vs_mix": same,
-        "latency_us": {"one_at_a_time_p50": float(np.percentile(lat_single, 50)),
-                       "one_at_a_time_p99": float(np.percentile(lat_single, 99)),
-                       "served_poisson_p50": float(np.percentile(lat_poisson, 50)),
-                       "served_poisson_p99": float(np.percentile(lat_poisson, 99)),
-                       "poisson_rate_qps": rate},
+        "config": {"workload": f"{a.batch_queries} filter + GROUP BY queries over resident {n}-row columns, "
+                               "rows/query log-uniform 1e4..5e7, cardinality log-uniform 10..1e6, int32/int64 keys, "
+                               "int64/f64 values", "lanes": a.lanes, "max_batch": a.max_batch},
+        **main_mix,
+        "small_query_mix": dict(small_mix, workload="same, rows/query log-uniform 1e4..1e6"),
         "gpu_launches": None,
     }
     return line

@@ -271,18 +271,29 @@ class Engine:
         ``where`` holds (column, cmp, literal) conjuncts. Returns None when the
         shape is declined (the reference's ``Ok(None)``)."""
         host_out = not all(v.is_cuda for v in table.values())
+        host_in = not any(v.is_cuda for v in table.values())
+        if host_in:
+            # All columns on the host: stream them through bolt_groupby_host
+            # (chunked upload overlapped with the aggregation).
+            pq = PreparedGroupby(self, dict(table), list(group_by), list(aggs), list(where), int(groups_hint),
+                                 out_cap, None)
+            r = self._run_groupby(self._lib.bolt_groupby_host, pq, flags, host_out, "GROUP BY (host columns)")
+            if r is not None or "row-order overflow check" not in self._lib.bolt_ctx_last_error(self._ctx).decode():
+                return r
         pq = self.prepare_groupby(table, group_by, aggs, where, groups_hint, out_cap)
+        return self._run_groupby(self._lib.bolt_groupby, pq, flags, host_out, "GROUP BY")
+
+    def _run_groupby(self, fn, pq: "PreparedGroupby", flags: int, host_out: bool, what: str):
         for _attempt in range(2):
-            st = self._lib.bolt_groupby(self._ctx, C.byref(pq.desc), C.byref(pq.out), flags | FLAG_PROFILE,
-                                        C.c_void_p(self.stream_handle))
+            st = fn(self._ctx, C.byref(pq.desc), C.byref(pq.out), flags | FLAG_PROFILE, C.c_void_p(self.stream_handle))
             if st == _abi.ERR_CAPACITY and pq.out.n_groups > pq.cap:
                 pq.realloc(int(pq.out.n_groups))
                 continue
-            if not self._check(st, "GROUP BY", decline_ok=True):
+            if not self._check(st, what, decline_ok=True):
                 return None
             self._lib.bolt_ctx_kernel_times(self._ctx, None, 1 << 20)
             return pq.result(host_out)
-        raise GpuCapacityError("GROUP BY: output capacity retry failed", _abi.ERR_CAPACITY)
+        raise GpuCapacityError(f"{what}: output capacity retry failed", _abi.ERR_CAPACITY)
 
     def execute_groupby(self, *args, **kw) -> GroupbyResult:
         r = self.try_execute_groupby(*args, **kw)
@@ -442,6 +453,16 @@ class Engine:
             self._lib.bolt_hash_join_release(self._ctx, table)
 
 
+def _to_pinned_host(c: Column) -> Column:
+    """Asynchronous device -> pinned host copy on the current stream (the
+    caller synchronises once for all columns)."""
+    def cp(t):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t, non_blocking=True)
+        return h
+    return Column(cp(c.data), c.dtype, cp(c.validity) if c.validity is not None else None, c.scale)
+
+
 class PreparedGroupby:
     """Descriptor + output columns of one GROUP BY through the C ABI. Keeps
     every buffer the descriptor points to alive."""
@@ -500,8 +521,9 @@ class PreparedGroupby:
         res = GroupbyResult([Engine._trim(c, g) for c in self.kout], [Engine._trim(c, g) for c in self.aout], g,
                             self.eng.last_device_ms, self.eng.last_launches)
         if host_out:
-            res.keys = [c.to("cpu") for c in res.keys]
-            res.aggs = [c.to("cpu") for c in res.aggs]
+            res.keys = [_to_pinned_host(c) for c in res.keys]
+            res.aggs = [_to_pinned_host(c) for c in res.aggs]
+            torch.cuda.current_stream(self.eng.device).synchronize()
         return res
 
 

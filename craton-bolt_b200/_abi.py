@@ -93,6 +93,8 @@ SIGNATURES = {
     "bolt_ctx_scratch_bytes": (C.c_uint64, [C.c_void_p]),
     "bolt_version": (C.c_char_p, []),
     "bolt_groupby": (C.c_int, [C.c_void_p, C.POINTER(GroupbyDesc), C.POINTER(GroupbyOut), C.c_uint32, C.c_void_p]),
+    "bolt_groupby_host": (C.c_int, [C.c_void_p, C.POINTER(GroupbyDesc), C.POINTER(GroupbyOut), C.c_uint32,
+                                    C.c_void_p]),
     "bolt_groupby_noalloc": (C.c_int, [C.POINTER(GroupbyDesc), C.POINTER(GroupbyOut), C.c_void_p, C.c_char_p,
                                        C.c_int32]),
     "bolt_groupby_autotune": (C.c_int, [C.c_void_p, C.POINTER(GroupbyDesc), C.POINTER(GroupbyOut), C.c_void_p,

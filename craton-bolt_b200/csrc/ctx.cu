@@ -183,6 +183,9 @@ void bolt_ctx_destroy(bolt_ctx* ctx) {
     for (uint32_t i = 0; i < bolt_ctx::STAGE_SLOTS; ++i)
         if (ctx->stage_use[i].ev) cudaEventDestroy(ctx->stage_use[i].ev);
     if (ctx->stage) cudaFreeHost(ctx->stage);
+    for (int i = 0; i < 2 * bolt_ctx::HOST_SLOTS + 1; ++i)
+        if (ctx->host_ev[i]) cudaEventDestroy(ctx->host_ev[i]);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     delete ctx;
 }
 

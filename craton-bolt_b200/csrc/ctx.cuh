@@ -52,6 +52,11 @@ struct bolt_ctx {
     // chunks per consumer warp (0 = the register kernel).
     struct GbTune { int32_t block, smem_shift, warp_agg, load_shift, smem_fill, staged; double ms; };
     std::unordered_map<uint64_t, GbTune> tune;
+    // Host-column GROUP BY (bolt_groupby_host): a copy stream and, per
+    // staging slot, "copied" / "consumed" events; created on first use.
+    static constexpr int HOST_SLOTS = 3;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t host_ev[2 * HOST_SLOTS + 1] = {};
 };
 
 namespace bolt {

@@ -309,8 +309,6 @@ __device__ __forceinline__ int s_find_insert(ull* sk, int log2, ull stored, uint
 // ---------------------------------------------------------------------------
 struct SpecGeneric {
     static constexpr bool generic = true;
-    static constexpr int n = 0;
-    __host__ __device__ static constexpr int kind(int) { return 0; }
 };
 template <int N, int K0, int K1 = 0, int K2 = 0, int K3 = 0>
 struct SpecK {
@@ -1477,7 +1475,10 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
 
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
     pl->shape = gb_shape_key(p, n, d->groups_hint);
-    bolt_ctx::GbTune tn{512, 1, 0, 2, 4, 0, 0.0};
+    // Untuned default: the register kernel for small inputs, the staged
+    // kernel (2 chunks per consumer warp) from 4M rows, where its pipeline
+    // fills.
+    bolt_ctx::GbTune tn{512, 1, 0, 2, 4, n >= (1ull << 22) ? 2 : 0, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
@@ -1590,7 +1591,8 @@ bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& pl, GbStagedLaunch* out
     }
 }
 
-bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
+// Allocates and zeroes the queries' tables and words and points the plans at them.
+static bolt_status gb_run_tables(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s) {
     if (nq <= 0) return BOLT_OK;
     // Tables and per-query words (occupancy, groups, status) in one zeroed region.
     std::vector<uint64_t> toff(nq);
@@ -1624,91 +1626,126 @@ bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t
         for (int s2 = 0; s2 < p.n_st; ++s2)
             if (p.st[s2].kind == K_SUM_I64) p.i64_bits = (uint32_t*)(w + 4);
     }
+    return BOLT_OK;
+}
 
-    // Aggregation.
-    if (nq == 1) {
-        GbPlan* pl = pls[0];
-        GbParams& p = pl->prm;
-        size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
-        const uint64_t tile = (uint64_t)pl->block * pl->u;
-        GbStagedLaunch stg;
-        const bool staged = gb_staged_layout(ctx, *pl, &stg);
-        AggKernel kfn;
-        int block = pl->block;
-        uint64_t tiles;
-        if (staged) {
-            kfn = staged_kernel_for(p.spec);
-            block = stg.block;
-            smem = stg.smem;
-            p.smem_log2 = stg.smem_log2;
-            p.smem_fill = stg.smem_log2 ? (uint32_t)(((1ull << stg.smem_log2) * (uint64_t)pl->tune.smem_fill) / 8) : 0;
-            p.tile_rows = stg.tile_rows;
-            p.n_stages = stg.n_stages;
-            p.stage_bytes = stg.stage_bytes;
-            p.chunks = pl->tune.staged;
-            uint32_t off = 0;
-            for (int c = 0; c < p.n_sc; ++c) {
-                p.sc_off[c] = off;
-                off += stg.tile_rows * (uint32_t)p.sc_w[c];
-            }
-            tiles = std::max<uint64_t>(p.n_rows / stg.tile_rows, 1);
-        } else {
-            kfn = agg_kernel_for(p.spec, p.n_st);
-            tiles = (p.n_rows + tile - 1) / tile;
+// Launches the aggregation of one query (the single-query kernels).
+static bolt_status gb_agg_one(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags) {
+    GbParams& p = pl->prm;
+    size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
+    const uint64_t tile = (uint64_t)pl->block * pl->u;
+    GbStagedLaunch stg;
+    const bool staged = gb_staged_layout(ctx, *pl, &stg);
+    AggKernel kfn;
+    int block = pl->block;
+    uint64_t tiles;
+    if (staged) {
+        kfn = staged_kernel_for(p.spec);
+        block = stg.block;
+        smem = stg.smem;
+        p.smem_log2 = stg.smem_log2;
+        p.smem_fill = stg.smem_log2 ? (uint32_t)(((1ull << stg.smem_log2) * (uint64_t)pl->tune.smem_fill) / 8) : 0;
+        p.tile_rows = stg.tile_rows;
+        p.n_stages = stg.n_stages;
+        p.stage_bytes = stg.stage_bytes;
+        p.chunks = pl->tune.staged;
+        uint32_t off = 0;
+        for (int c = 0; c < p.n_sc; ++c) {
+            p.sc_off[c] = off;
+            off += stg.tile_rows * (uint32_t)p.sc_w[c];
         }
-        int per_sm = 1;
-        BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
-            per_sm = 1;
-        uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
-        if (pl->grid > 0) grid = std::min<uint64_t>(grid, (uint64_t)pl->grid);
-        pl->grid = (int)grid;
-        if (p.n_rows > 0) {
-            kernel_mark_begin(ctx, flags, s);
-            kfn<<<pl->grid, block, smem, s>>>(p);
-            ctx->last_launches++;
-            kernel_mark_end(ctx, flags, s);
-        }
+        tiles = std::max<uint64_t>(p.n_rows / stg.tile_rows, 1);
     } else {
-        // One compiled row loop for the whole batch: the queries' common
-        // layout, else the generic loop.
-        int u = 4, max_st = 0, spec = pls[0]->prm.spec;
-        size_t smem = 0;
-        for (int q = 0; q < nq; ++q) {
-            max_st = std::max(max_st, (int)pls[q]->prm.n_st);
-            if (pls[q]->prm.spec != spec) spec = 0;
-            smem = std::max<size_t>(smem, (size_t)pls[q]->smem_entries * 8 * (size_t)pls[q]->prm.slot_words);
-        }
-        if (spec == 0 && max_st > 4) u = 2;
-        const BatchKernel kfn = batch_kernel_for(spec, max_st);
-        const uint32_t item_tiles = 4;
-        std::vector<GbParams> prms(nq);
-        std::vector<uint32_t> begins(nq + 1);
-        uint64_t items = 0;
-        const uint64_t tile = 512ull * u * item_tiles;
-        for (int q = 0; q < nq; ++q) {
-            prms[q] = pls[q]->prm;
-            begins[q] = (uint32_t)items;
-            items += (pls[q]->prm.n_rows + tile - 1) / tile;
-        }
-        begins[nq] = (uint32_t)items;
-        if (items >= (1ull << 32)) return fail(ctx, BOLT_DECLINE, "batched GROUP BY: too many row tiles");
-        GbParams* d_prms = (GbParams*)arena_alloc(ctx, sizeof(GbParams) * nq);
-        uint32_t* d_begins = (uint32_t*)arena_alloc(ctx, 4ull * (nq + 1) + 64);
-        if (!d_prms || !d_begins) return fail(ctx, BOLT_ERR_CAPACITY, "batched GROUP BY: scratch arena too small");
-        uint32_t* counter = d_begins + nq + 1;
-        bolt_status st = stage_upload(ctx, s, d_prms, prms.data(), sizeof(GbParams) * nq);
-        if (st == BOLT_OK) st = stage_upload(ctx, s, d_begins, begins.data(), 4ull * (nq + 1));
+        kfn = agg_kernel_for(p.spec, p.n_st);
+        tiles = (p.n_rows + tile - 1) / tile;
+    }
+    int per_sm = 1;
+    BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
+    if (pl->grid > 0) grid = std::min<uint64_t>(grid, (uint64_t)pl->grid);
+    pl->grid = (int)grid;
+    if (p.n_rows > 0) {
+        kernel_mark_begin(ctx, flags, s);
+        kfn<<<pl->grid, block, smem, s>>>(p);
+        ctx->last_launches++;
+        kernel_mark_end(ctx, flags, s);
+    }
+    return BOLT_OK;
+}
+
+// One persistent launch over a group of queries that share a compiled layout.
+static bolt_status gb_agg_batch(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
+    // One compiled row loop for the whole batch: the queries' common
+    // layout, else the generic loop.
+    int u = 4, max_st = 0, spec = pls[0]->prm.spec;
+    size_t smem = 0;
+    for (int q = 0; q < nq; ++q) {
+        max_st = std::max(max_st, (int)pls[q]->prm.n_st);
+        if (pls[q]->prm.spec != spec) spec = 0;
+        smem = std::max<size_t>(smem, (size_t)pls[q]->smem_entries * 8 * (size_t)pls[q]->prm.slot_words);
+    }
+    if (spec == 0 && max_st > 4) u = 2;
+    const BatchKernel kfn = batch_kernel_for(spec, max_st);
+    const uint32_t item_tiles = 4;
+    std::vector<GbParams> prms(nq);
+    std::vector<uint32_t> begins(nq + 1);
+    uint64_t items = 0;
+    const uint64_t tile = 512ull * u * item_tiles;
+    for (int q = 0; q < nq; ++q) {
+        prms[q] = pls[q]->prm;
+        begins[q] = (uint32_t)items;
+        items += (pls[q]->prm.n_rows + tile - 1) / tile;
+    }
+    begins[nq] = (uint32_t)items;
+    if (items >= (1ull << 32)) return fail(ctx, BOLT_DECLINE, "batched GROUP BY: too many row tiles");
+    GbParams* d_prms = (GbParams*)arena_alloc(ctx, sizeof(GbParams) * nq);
+    uint32_t* d_begins = (uint32_t*)arena_alloc(ctx, 4ull * (nq + 1) + 64);
+    if (!d_prms || !d_begins) return fail(ctx, BOLT_ERR_CAPACITY, "batched GROUP BY: scratch arena too small");
+    uint32_t* counter = d_begins + nq + 1;
+    bolt_status st = stage_upload(ctx, s, d_prms, prms.data(), sizeof(GbParams) * nq);
+    if (st == BOLT_OK) st = stage_upload(ctx, s, d_begins, begins.data(), 4ull * (nq + 1));
+    if (st != BOLT_OK) return st;
+    BOLT_CUDA(ctx, cudaMemsetAsync(counter, 0, 4, s));
+    if (items) {
+        kernel_mark_begin(ctx, flags, s);
+        st = launch_batch_agg(ctx, s, kfn, d_prms, d_begins, nq, (uint32_t)items, item_tiles, counter, smem, 512);
+        kernel_mark_end(ctx, flags, s);
         if (st != BOLT_OK) return st;
-        BOLT_CUDA(ctx, cudaMemsetAsync(counter, 0, 4, s));
-        if (items) {
-            kernel_mark_begin(ctx, flags, s);
-            st = launch_batch_agg(ctx, s, kfn, d_prms, d_begins, nq, (uint32_t)items, item_tiles, counter, smem, 512);
-            kernel_mark_end(ctx, flags, s);
+    }
+    return BOLT_OK;
+}
+
+// Queries with at least this many rows are launched alone in a batch: at that
+// size a launch of their own costs little, and they get the single-query
+// kernels (the staged kernel among them).
+constexpr uint64_t BATCH_ALONE_ROWS = 1ull << 21;
+
+// Launches the aggregation of every query into its table: one query alone;
+// in a batch, large queries alone and the others grouped by compiled layout,
+// one persistent launch per group.
+static bolt_status gb_run_aggregate(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
+    if (nq == 1) return gb_agg_one(ctx, pls[0], s, flags);
+    std::vector<GbPlan*> groups[8];
+    for (int q = 0; q < nq; ++q) {
+        if (pls[q]->prm.n_rows >= BATCH_ALONE_ROWS) {
+            bolt_status st = gb_agg_one(ctx, pls[q], s, flags);
             if (st != BOLT_OK) return st;
+        } else {
+            groups[std::min(std::max(pls[q]->prm.spec, 0), 7)].push_back(pls[q]);
         }
     }
+    for (auto& g : groups) {
+        if (g.empty()) continue;
+        bolt_status st = gb_agg_batch(ctx, g.data(), (int)g.size(), s, flags);
+        if (st != BOLT_OK) return st;
+    }
+    return BOLT_OK;
+}
 
+// Finalizes every query's table into its output columns.
+static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s) {
     // Finalize: small tables one CTA each; large tables through batched
     // compaction, a segmented radix sort and a batched gather.
     std::vector<GbFinal> small, large;
@@ -1775,6 +1812,14 @@ bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t
     }
     BOLT_CUDA(ctx, cudaGetLastError());
     return BOLT_OK;
+}
+
+bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
+    if (nq <= 0) return BOLT_OK;
+    bolt_status st = gb_run_tables(ctx, pls, nq, s);
+    if (st == BOLT_OK) st = gb_run_aggregate(ctx, pls, nq, s, flags);
+    if (st == BOLT_OK) st = gb_run_finalize(ctx, pls, nq, s);
+    return st;
 }
 
 }  // namespace bolt
@@ -1880,7 +1925,196 @@ static bolt_status gb_single(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_gro
     return fail(ctx, BOLT_ERR_CAPACITY, "%s: table growth did not converge", op);
 }
 
+// Adds `delta` to every column pointer of `p` that lies in [lo, hi).
+static void gb_rebase(GbParams& p, uintptr_t lo, uintptr_t hi, ptrdiff_t delta) {
+    auto fix = [&](const void*& q) {
+        const uintptr_t v = reinterpret_cast<uintptr_t>(q);
+        if (v >= lo && v < hi) q = reinterpret_cast<const void*>(v + delta);
+    };
+    auto fixv = [&](const uint8_t*& q) {
+        const void* t = q;
+        fix(t);
+        q = static_cast<const uint8_t*>(t);
+    };
+    for (int k = 0; k < 2; ++k) {
+        fix(p.kcol[k]);
+        fixv(p.kvalid[k]);
+    }
+    for (int q = 0; q < GB_MAX_PREDS; ++q) {
+        fix(p.pred[q].col);
+        fixv(p.pred[q].valid);
+    }
+    for (int s2 = 0; s2 < GB_MAX_STATES; ++s2) {
+        fix(p.st[s2].col);
+        fixv(p.st[s2].valid);
+    }
+    for (int c = 0; c < GB_MAX_SC; ++c) fix(p.sc_col[c]);
+}
+
+// GROUP BY over host-resident columns. The rows go to the device in chunks
+// on the context's copy stream, into a ring of staging slots in the scratch
+// arena, while the aggregation kernel folds the previous chunks into the one
+// table on the caller's stream: the host -> device transfer and the
+// aggregation overlap, and no column is ever resident in full.
+static bolt_status gb_host(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_groupby_out* out, uint32_t flags,
+                           cudaStream_t s) {
+    const char* op = "GROUP BY (host columns)";
+    if (flags & BOLT_FLAG_ASYNC) return fail(ctx, BOLT_ERR_INVALID, "%s: BOLT_FLAG_ASYNC is not supported", op);
+    if (!d->cols || d->n_cols <= 0 || d->n_cols > 64 || !d->key_cols || d->n_keys < 1 || d->n_keys > 2 ||
+        d->n_preds < 0 || d->n_preds > GB_MAX_PREDS || d->n_aggs < 0 || (d->n_preds && !d->preds) ||
+        (d->n_aggs && !d->aggs))
+        return fail(ctx, BOLT_ERR_INVALID, "%s: bad descriptor", op);
+    bool used[64] = {};
+    auto use = [&](int i) {
+        if (i < 0 || i >= d->n_cols) return false;
+        used[i] = true;
+        return true;
+    };
+    for (int k = 0; k < d->n_keys; ++k)
+        if (!use(d->key_cols[k])) return fail(ctx, BOLT_ERR_INVALID, "%s: key column out of range", op);
+    for (int q = 0; q < d->n_preds; ++q)
+        if (!use(d->preds[q].col)) return fail(ctx, BOLT_ERR_INVALID, "%s: WHERE column out of range", op);
+    for (int a = 0; a < d->n_aggs; ++a)
+        if (d->aggs[a].op != BOLT_AGG_COUNT_STAR && !use(d->aggs[a].input_col))
+            return fail(ctx, BOLT_ERR_INVALID, "%s: aggregate column out of range", op);
+    const uint64_t n = d->cols[d->key_cols[0]].len;
+    uint64_t row_bytes = 0;
+    for (int i = 0; i < d->n_cols; ++i) {
+        if (!used[i]) continue;
+        const int w = dtype_width(d->cols[i].dtype);
+        if (w == 0 || !d->cols[i].data) return fail(ctx, BOLT_ERR_INVALID, "%s: column %d has no data", op, i);
+        if (d->cols[i].len < n) return fail(ctx, BOLT_ERR_INVALID, "%s: column %d shorter than the key", op, i);
+        row_bytes += (uint64_t)w + (d->cols[i].validity ? 1 : 0);
+    }
+    constexpr int NB = bolt_ctx::HOST_SLOTS;
+    if (!ctx->copy_stream) {
+        BOLT_CUDA(ctx, cudaSetDevice(ctx->device));
+        BOLT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2 * NB + 1; ++i)
+            BOLT_CUDA(ctx, cudaEventCreateWithFlags(&ctx->host_ev[i], cudaEventDisableTiming));
+    }
+    cudaEvent_t* copied = ctx->host_ev;
+    cudaEvent_t* consumed = ctx->host_ev + NB;
+    cudaEvent_t start = ctx->host_ev[2 * NB];
+    // Whatever leaves this function, the copies that read the caller's host
+    // buffers have finished.
+    struct CopyDrain {
+        cudaStream_t cs;
+        ~CopyDrain() { cudaStreamSynchronize(cs); }
+    } drain{ctx->copy_stream};
+
+    int mode = 0;
+    uint64_t cap_override = 0;
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        bolt_status st = call_begin(ctx, flags, s);
+        if (st != BOLT_OK) return st;
+        // Chunk rows: a multiple of 64 (whole validity bytes), 4M at most,
+        // the ring using at most a quarter of the free arena.
+        const uint64_t free_b = ctx->arena_bytes - ctx->arena_used;
+        uint64_t R = std::min<uint64_t>(4ull << 20, (n + 63) & ~63ull);
+        while (R > 64 && (uint64_t)NB * (R * row_bytes + 256ull * 2 * d->n_cols) > free_b / 4) R = (R / 2 + 63) & ~63ull;
+        R = std::max<uint64_t>(R, 64);
+        // Slot layout: every used column's data and validity at fixed offsets.
+        std::vector<uint64_t> doff(d->n_cols, 0), voff(d->n_cols, 0);
+        uint64_t stride = 0;
+        for (int i = 0; i < d->n_cols; ++i) {
+            if (!used[i]) continue;
+            doff[i] = stride;
+            stride += (R * (uint64_t)dtype_width(d->cols[i].dtype) + 255) & ~255ull;
+            if (d->cols[i].validity) {
+                voff[i] = stride;
+                stride += (R / 8 + 255) & ~255ull;
+            }
+        }
+        char* ring = (char*)arena_alloc(ctx, stride * NB);
+        if (!ring) return fail(ctx, BOLT_ERR_CAPACITY, "%s: scratch arena too small for the staging ring", op);
+        std::vector<bolt_col_view> dcols(d->cols, d->cols + d->n_cols);
+        for (int i = 0; i < d->n_cols; ++i) {
+            if (!used[i]) continue;
+            dcols[i].data = ring + doff[i];
+            dcols[i].validity = d->cols[i].validity ? reinterpret_cast<const uint8_t*>(ring + voff[i]) : nullptr;
+        }
+        bolt_groupby_desc dd = *d;
+        dd.cols = dcols.data();
+        GbPlan pl;
+        st = gb_plan(ctx, &dd, out, 0, n, flags, mode, cap_override, &pl);
+        if (st != BOLT_OK) return st;
+        pl.fin.n_groups_user = nullptr;
+        GbPlan* one = &pl;
+        st = gb_run_tables(ctx, &one, 1, s);
+        if (st != BOLT_OK) return st;
+        const GbParams base = pl.prm;
+        // The ring may still be read by an earlier call's kernels on `s`.
+        BOLT_CUDA(ctx, cudaEventRecord(start, s));
+        BOLT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, start, 0));
+        const uint64_t chunks = (n + R - 1) / R;
+        for (uint64_t c = 0; c < chunks; ++c) {
+            const int k = (int)(c % NB);
+            const uint64_t r0 = c * R;
+            const uint64_t rows = std::min<uint64_t>(R, n - r0);
+            if (c >= (uint64_t)NB) BOLT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, consumed[k], 0));
+            char* slot = ring + (uint64_t)k * stride;
+            for (int i = 0; i < d->n_cols; ++i) {
+                if (!used[i]) continue;
+                const uint64_t w = (uint64_t)dtype_width(d->cols[i].dtype);
+                BOLT_CUDA(ctx, cudaMemcpyAsync(slot + doff[i], static_cast<const char*>(d->cols[i].data) + r0 * w,
+                                               rows * w, cudaMemcpyHostToDevice, ctx->copy_stream));
+                if (d->cols[i].validity)
+                    BOLT_CUDA(ctx, cudaMemcpyAsync(slot + voff[i], d->cols[i].validity + r0 / 8, (rows + 7) / 8,
+                                                   cudaMemcpyHostToDevice, ctx->copy_stream));
+            }
+            BOLT_CUDA(ctx, cudaEventRecord(copied[k], ctx->copy_stream));
+            BOLT_CUDA(ctx, cudaStreamWaitEvent(s, copied[k], 0));
+            pl.prm = base;
+            gb_rebase(pl.prm, reinterpret_cast<uintptr_t>(ring), reinterpret_cast<uintptr_t>(ring) + stride,
+                      (ptrdiff_t)((uint64_t)k * stride));
+            pl.prm.row_begin = 0;
+            pl.prm.n_rows = rows;
+            pl.grid = 0;
+            st = gb_run_aggregate(ctx, &one, 1, s, flags);
+            if (st != BOLT_OK) return st;
+            BOLT_CUDA(ctx, cudaEventRecord(consumed[k], s));
+        }
+        pl.prm = base;
+        st = gb_run_finalize(ctx, &one, 1, s);
+        if (st != BOLT_OK) return st;
+        st = call_end(ctx, flags, s);
+        if (st != BOLT_OK) return st;
+        uint32_t f = 0;
+        st = read_status(ctx, s, 0, &f);
+        if (st != BOLT_OK) return st;
+        ull w[5] = {0, 0, 0, 0, 0};
+        BOLT_CUDA(ctx, cudaMemcpy(w, pl.words, sizeof w, cudaMemcpyDeviceToHost));
+        out->n_groups = w[2];
+        if (f == 0 && base.i64_bits && (uint32_t)w[4] + (uint32_t)ceil_log2_u64(n + 1) >= 63)
+            return fail(ctx, BOLT_DECLINE,
+                        "%s: SUM(Int64) inputs large enough to need the row-order overflow check; run it on device "
+                        "columns (bolt_groupby)", op);
+        if (f & (ST_FLAG_GROW | ST_FLAG_SPILL)) {
+            if (flags & BOLT_FLAG_FORCE_SHMEM)
+                return fail(ctx, BOLT_ERR_SPILL, "partition_reduce spill: shared-memory tier overflow");
+            cap_override = pl.cap * 8;
+            continue;
+        }
+        if (f & (ST_FLAG_RANGE | ST_FLAG_DECRANGE)) {
+            if (f & ST_FLAG_RANGE) mode |= GB_MODE_F64_ATOMIC;
+            if (f & ST_FLAG_DECRANGE) mode |= GB_MODE_WIDE_DEC;
+            continue;
+        }
+        if (f & ST_FLAG_DECOVERFLOW)
+            return fail(ctx, BOLT_ERR_OVERFLOW, "SUM(Decimal128) precision overflow: accumulator exceeds i128 range");
+        return flags_to_status(ctx, f, op);
+    }
+    return fail(ctx, BOLT_ERR_CAPACITY, "%s: table growth did not converge", op);
+}
+
 }  // namespace bolt
+
+extern "C" bolt_status bolt_groupby_host(bolt_ctx* ctx, const bolt_groupby_desc* desc, bolt_groupby_out* out,
+                                         uint32_t flags, bolt_stream stream) {
+    if (!ctx || !desc || !out) return BOLT_ERR_INVALID;
+    return gb_host(ctx, desc, out, flags, (cudaStream_t)stream);
+}
 
 extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc, bolt_groupby_out* out,
                                     uint32_t flags, bolt_stream stream) {

@@ -195,6 +195,20 @@ typedef struct {
 bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc,
                          bolt_groupby_out* out, uint32_t flags, bolt_stream stream);
 
+/* GROUP BY over HOST-resident columns: every data / validity pointer of
+ * desc->cols is host memory (pinned memory lets the copies overlap); the
+ * outputs are device columns, exactly as for bolt_groupby. Replaces the
+ * reference's host RecordBatch path, which uploads each column before its
+ * kernels (src/exec/groupby.rs:295-833; the uploads are ~78 % of the h2o q1
+ * time, groupby.rs:270-272). Here the rows stream to the device in chunks on
+ * a second stream while the aggregation folds the chunks already there, so
+ * transfer and aggregation overlap and no column is resident in full.
+ * Always synchronises (BOLT_FLAG_ASYNC -> BOLT_ERR_INVALID). A query whose
+ * SUM(Int64) needs the row-order overflow check returns BOLT_DECLINE: run it
+ * on device columns through bolt_groupby. */
+bolt_status bolt_groupby_host(bolt_ctx* ctx, const bolt_groupby_desc* desc,
+                              bolt_groupby_out* out, uint32_t flags, bolt_stream stream);
+
 /* GROUP BY that allocates no device memory. No counterpart in the
  * reference. For callers that may not call cudaMalloc / cudaFree at all (an
  * engine whose own pool owns all of HBM, or a latency-critical loop where an

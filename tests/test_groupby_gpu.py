@@ -314,6 +314,54 @@ def test_groupby_host_inputs_end_to_end(bolt, engine, oracle):
     compare_groupby(res, orc, ["i32"], [("sum", "v"), ("count_star", None)], ["i64", None])
 
 
+def test_groupby_host_columns_streamed_in_chunks(bolt, engine, oracle):
+    """Host columns through bolt_groupby_host: more rows than one 4M-row
+    chunk (plus a remainder), a nullable single key, nullable values and a
+    WHERE; equal to the oracle and bit-identical to the device-column path."""
+    rng = np.random.default_rng(41)
+    n = 9_000_013
+    k = rng.integers(-20000, 20000, n).astype(np.int32)
+    kv = rng.random(n) > 0.001
+    v = rng.integers(-10**9, 10**9, n).astype(np.int64)
+    vv = rng.random(n) > 0.05
+    d = rng.normal(0, 100, n)
+    f = rng.integers(0, 100, n).astype(np.int32)
+    cols = {"k": (k, bitmap(kv), "i32", 0), "v": (v, bitmap(vv), "i64", 0), "d": (d, None, "f64", 0),
+            "f": (f, None, "i32", 0)}
+    aggs = [("sum", "v"), ("count", "v"), ("avg", "d"), ("max", "d"), ("count_star", None)]
+    where = [("f", ">=", 20)]
+    host = {name: bolt.Column(torch.from_numpy(a).pin_memory(), dt,
+                              torch.from_numpy(vb).pin_memory() if vb is not None else None, sc)
+            for name, (a, vb, dt, sc) in cols.items()}
+    res = engine.execute_groupby(host, ["k"], aggs, where=where, groups_hint=40_000)
+    assert not res.keys[0].is_cuda
+    hcols = {name: oracle.HostCol(a, dt, vb, sc) for name, (a, vb, dt, sc) in cols.items()}
+    orc = oracle.groupby(hcols, ["k"], aggs, where=where)
+    compare_groupby(res, orc, ["i32"], aggs, ["i64", "i64", "f64", "f64", None])
+    dev, _ = tables(bolt, oracle, cols)
+    r2 = engine.execute_groupby(dev, ["k"], aggs, where=where, groups_hint=40_000)
+    assert r2.n_groups == res.n_groups
+    for x, y in zip(res.keys + res.aggs, r2.keys + r2.aggs):
+        np.testing.assert_array_equal(x.valid_mask(), y.valid_mask())
+        xd, yd = x.numpy(), y.numpy()
+        if x.dtype == "f64":
+            xd, yd = xd.view(np.int64), yd.view(np.int64)
+        np.testing.assert_array_equal(xd[x.valid_mask()], yd[y.valid_mask()])
+
+
+def test_groupby_host_columns_row_order_check_falls_back(bolt, engine, oracle):
+    """A SUM(Int64) that needs the row-order overflow check is declined by the
+    streamed path and run on device columns instead: same error as bolt_groupby."""
+    k = np.array([0, 1, 0, 1, 0, 1, 0, 1], np.int32)
+    v = np.array([s * 2**62 for s in (1, 1, -1, -1) for _ in range(2)], np.int64)
+    host = {"k": bolt.col(k, "i32"), "v": bolt.col(v, "i64")}
+    with pytest.raises(bolt.TypeError_):
+        engine.execute_groupby(host, ["k"], [("sum", "v")])
+    v2 = np.array([s * 2**62 for s in (1, -1, 1, -1) for _ in range(2)], np.int64)
+    res = engine.execute_groupby({"k": bolt.col(k, "i32"), "v": bolt.col(v2, "i64")}, ["k"], [("sum", "v")])
+    assert res.aggs[0].numpy().tolist() == [0, 0]
+
+
 def test_autotune_keeps_results_and_persists(bolt, engine, oracle, tmp_path):
     cols = filtered_config(1_000_000, 100_000, seed=13)
     dev, host = tables(bolt, oracle, cols)
