@@ -18,20 +18,38 @@ namespace bolt {
 namespace {
 
 constexpr int CP_BLOCK = 256;
-constexpr int CP_ITEMS = 8;
-constexpr int CP_TILE = CP_BLOCK * CP_ITEMS;
 constexpr int CP_NW = CP_BLOCK / 32;
+// Rows per thread: 8 when columns are read straight from global memory, 4
+// when they are staged (smaller tiles keep more CTAs resident per SM).
+constexpr int CP_ITEMS_DIRECT = 8;
+constexpr int CP_ITEMS_STAGED = 4;
+// Largest staged tile (bytes of shared memory per CTA).
+constexpr uint32_t CP_STAGE_MAX = 48u << 10;
 constexpr ull LB_AGG = 1ull << 62;
 constexpr ull LB_INC = 2ull << 62;
 constexpr ull LB_VAL = (1ull << 62) - 1;
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
+constexpr int LB_WINDOW = 8;  // look-back words read per round trip
 
 struct CpArgs {
     CompactSpec sp;
     ull* lookback;
     uint32_t* tile_ctr;
     uint32_t* status;
+    uint32_t soff[CP_MAX_COLS];  // staged kernel: byte offset of each column's tile in shared memory
 };
+
+// Asynchronous global -> shared copy of one element (4, 8 or 16 bytes; both
+// addresses aligned to the size), cached in L1 so the predicate's loads of
+// the same rows hit.
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, int width) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    switch (width) {
+    case 4: asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory"); break;
+    case 8: asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory"); break;
+    default: asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory"); break;
+    }
+}
 
 __device__ __forceinline__ bool cp_pred(const CompactPred& d, uint64_t r) {
     if (!bit_valid(d.valid, r)) return false;
@@ -57,7 +75,15 @@ __device__ __forceinline__ bool cp_pred(const CompactPred& d, uint64_t r) {
     }
 }
 
+// STAGED: every thread first issues asynchronous copies of its rows of every
+// output column into shared memory, so the column reads are in flight while
+// the predicate is evaluated and the tile's offset is looked back; the
+// scatter then reads them back (each thread only its own rows).
+template <bool STAGED>
 __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant__ CpArgs a) {
+    constexpr int CP_ITEMS = STAGED ? CP_ITEMS_STAGED : CP_ITEMS_DIRECT;
+    constexpr int CP_TILE = CP_BLOCK * CP_ITEMS;
+    extern __shared__ __align__(16) unsigned char cp_stage[];
     __shared__ uint32_t s_tile;
     __shared__ uint32_t cnt[CP_ITEMS][CP_NW];
     __shared__ ull s_base;
@@ -70,6 +96,20 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
     if (tile >= ntiles) return;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t base = (uint64_t)tile * CP_TILE;
+    if (STAGED) {
+#pragma unroll
+        for (int j = 0; j < CP_ITEMS; ++j) {
+            const uint64_t e = base + (uint64_t)j * CP_BLOCK + threadIdx.x;
+            if (e >= n) continue;
+            const uint32_t slot = (uint32_t)j * CP_BLOCK + threadIdx.x;
+            for (int c = 0; c < sp.n_cols; ++c) {
+                const int wd = sp.col[c].width;
+                cp_async_elem(cp_stage + a.soff[c] + slot * (uint32_t)wd,
+                              static_cast<const unsigned char*>(sp.col[c].in) + e * (uint64_t)wd, wd);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
 
     uint32_t keep = 0;  // bit j: element base + j*BLOCK + tid is kept
 #pragma unroll
@@ -112,22 +152,38 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
                 *reinterpret_cast<volatile ull*>(my) = LB_INC | local;
             } else {
                 *reinterpret_cast<volatile ull*>(my) = LB_AGG | local;
+                // Look back LB_WINDOW words per round trip: sum aggregates
+                // until an inclusive prefix.
                 int64_t t = (int64_t)tile - 1;
                 uint32_t spins = 0;
                 while (t >= 0) {
-                    const ull v2 = ld_volatile(a.lookback + t);
-                    const ull st = v2 >> 62;
-                    if (st == 0) {
+                    const int cnt = (t + 1) < LB_WINDOW ? (int)(t + 1) : LB_WINDOW;
+                    ull v[LB_WINDOW];
+#pragma unroll
+                    for (int i = 0; i < LB_WINDOW; ++i) v[i] = i < cnt ? ld_volatile(a.lookback + (t - i)) : 0ull;
+                    int used = 0;
+                    bool done = false, stalled = false;
+#pragma unroll
+                    for (int i = 0; i < LB_WINDOW; ++i) {
+                        if (done || stalled || i >= cnt) continue;
+                        const ull st = v[i] >> 62;
+                        if (st == 0) {
+                            stalled = true;
+                            continue;
+                        }
+                        excl += v[i] & LB_VAL;
+                        ++used;
+                        if (st == 2) done = true;
+                    }
+                    if (done) break;
+                    t -= used;
+                    if (stalled) {
                         if (++spins > SPIN_LIMIT) {
                             atomicOr(a.status, ST_FLAG_TIMEOUT);
                             break;
                         }
                         if (spins > 4) __nanosleep(64);
-                        continue;
                     }
-                    excl += v2 & LB_VAL;
-                    if (st == 2) break;
-                    --t;
                 }
                 *reinterpret_cast<volatile ull*>(my) = LB_INC | (excl + local);
             }
@@ -140,6 +196,7 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
         }
     }
     __syncthreads();
+    if (STAGED) asm volatile("cp.async.wait_all;" ::: "memory");
     const ull tbase = s_base;
 #pragma unroll
     for (int j = 0; j < CP_ITEMS; ++j) {
@@ -148,12 +205,22 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
         if (!((keep >> j) & 1u)) continue;
         const ull pos = tbase + cnt[j][w] + __popc(b & lanemask_lt());
         if (pos >= sp.out_cap) continue;
+        const uint32_t slot = (uint32_t)j * CP_BLOCK + threadIdx.x;
         for (int c = 0; c < sp.n_cols; ++c) {
             const CompactCol& col = sp.col[c];
-            switch (col.width) {
-            case 4: ((uint32_t*)col.out)[pos] = __ldg((const uint32_t*)col.in + e); break;
-            case 8: ((ull*)col.out)[pos] = __ldg((const ull*)col.in + e); break;
-            default: ((ulonglong2*)col.out)[pos] = __ldg((const ulonglong2*)col.in + e); break;
+            if (STAGED) {
+                const unsigned char* src = cp_stage + a.soff[c] + slot * (uint32_t)col.width;
+                switch (col.width) {
+                case 4: ((uint32_t*)col.out)[pos] = *reinterpret_cast<const uint32_t*>(src); break;
+                case 8: ((ull*)col.out)[pos] = *reinterpret_cast<const ull*>(src); break;
+                default: ((ulonglong2*)col.out)[pos] = *reinterpret_cast<const ulonglong2*>(src); break;
+                }
+            } else {
+                switch (col.width) {
+                case 4: ((uint32_t*)col.out)[pos] = __ldg((const uint32_t*)col.in + e); break;
+                case 8: ((ull*)col.out)[pos] = __ldg((const ull*)col.in + e); break;
+                default: ((ulonglong2*)col.out)[pos] = __ldg((const ulonglong2*)col.in + e); break;
+                }
             }
             if (col.out_valid && bit_valid(col.in_valid, e)) set_bit_atomic(col.out_valid, pos, true);
         }
@@ -166,7 +233,21 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
 bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& spec) {
     CpArgs a{};
     a.sp = spec;
-    const uint64_t ntiles = (spec.n + CP_TILE - 1) / CP_TILE;
+    // Stage the columns when a tile of them fits the budget and every input
+    // is aligned to its width (the asynchronous copies need both).
+    uint32_t row_w = 0;
+    bool staged = spec.n_cols > 0;
+    for (int c = 0; c < spec.n_cols; ++c) {
+        const int wd = spec.col[c].width;
+        staged = staged && (wd == 4 || wd == 8 || wd == 16) &&
+                 reinterpret_cast<uintptr_t>(spec.col[c].in) % (uintptr_t)wd == 0;
+        a.soff[c] = row_w * (uint32_t)(CP_BLOCK * CP_ITEMS_STAGED);
+        row_w += (uint32_t)wd;
+    }
+    const uint32_t stage_bytes = row_w * (uint32_t)(CP_BLOCK * CP_ITEMS_STAGED);
+    staged = staged && stage_bytes <= CP_STAGE_MAX;
+    const uint64_t tile_rows = (uint64_t)CP_BLOCK * (staged ? CP_ITEMS_STAGED : CP_ITEMS_DIRECT);
+    const uint64_t ntiles = (spec.n + tile_rows - 1) / tile_rows;
     a.lookback = (ull*)arena_alloc(ctx, (ntiles + 1) * 8);
     a.tile_ctr = (uint32_t*)arena_alloc(ctx, 64);
     if (!a.lookback || !a.tile_ctr) return fail(ctx, BOLT_ERR_CAPACITY, "compaction: scratch arena too small");
@@ -181,7 +262,13 @@ bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& sp
         const uint64_t rows = spec.out_cap < spec.n ? spec.out_cap : spec.n;
         if (spec.col[c].out_valid) BOLT_CUDA(ctx, cudaMemsetAsync(spec.col[c].out_valid, 0, (rows + 7) / 8, s));
     }
-    compact_kernel<<<(unsigned)ntiles, CP_BLOCK, 0, s>>>(a);
+    if (staged) {
+        BOLT_CUDA(ctx, cudaFuncSetAttribute(compact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)stage_bytes));
+        compact_kernel<true><<<(unsigned)ntiles, CP_BLOCK, stage_bytes, s>>>(a);
+    } else {
+        compact_kernel<false><<<(unsigned)ntiles, CP_BLOCK, 0, s>>>(a);
+    }
     ctx->last_launches++;
     BOLT_CUDA(ctx, cudaGetLastError());
     return BOLT_OK;

@@ -6,7 +6,7 @@
 //   * one histogram kernel reads the keys once and counts all digit
 //     positions of every segment (8-bit digits: 4 passes for 32-bit keys,
 //     8 for 64-bit);
-//   * one kernel per digit: tiles of 4096 keys are taken in arrival order
+//   * one kernel per digit: tiles of 3072 keys are taken in arrival order
 //     from a flattened (segment, tile) list, ranked per warp with
 //     __match_any_sync (stable: element order within a warp's segment of the
 //     tile, warps in order), their digit counts chained across the segment's
@@ -27,13 +27,14 @@ namespace bolt {
 namespace {
 
 constexpr int SORT_BLOCK = 256;
-constexpr int SORT_ITEMS = 16;
+constexpr int SORT_ITEMS = 12;
 constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
 constexpr int HIST_CHUNK = 16384;
 constexpr uint32_t LB_AGG = 1u << 30;
 constexpr uint32_t LB_INC = 2u << 30;
 constexpr uint32_t LB_VAL = (1u << 30) - 1;
 constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+constexpr int LB_WINDOW = 8;  // look-back words read per round trip
 
 template <typename K> struct KeyTraits;
 template <> struct KeyTraits<uint32_t> { static constexpr int NPASS = 4; };
@@ -192,16 +193,19 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(SortArgs a) {
 }
 
 template <typename K>
-__global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p) {
+__global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, int p) {
     constexpr int NW = SORT_BLOCK / 32;
     __shared__ uint32_t s_item;
     __shared__ uint32_t warp_hist[NW][256];
     __shared__ uint32_t tile_off[256];
     __shared__ uint32_t gstart[256];
     __shared__ uint32_t wsum[8];
+    // Staged tile: keys, payloads and the digit of every position
+    // (3 CTAs of 256 threads per SM).
     extern __shared__ __align__(16) unsigned char dyn[];
     K* stage_key = reinterpret_cast<K*>(dyn);
     uint32_t* stage_pay = reinterpret_cast<uint32_t*>(dyn + sizeof(K) * SORT_TILE);
+    uint8_t* stage_dig = dyn + (sizeof(K) + 4) * SORT_TILE;
 
     if (threadIdx.x == 0) s_item = atomicAdd(&a.tile_ctr[p], 1u);
     for (int i = threadIdx.x; i < NW * 256; i += SORT_BLOCK) (&warp_hist[0][0])[i] = 0;
@@ -271,45 +275,18 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
     }
     __syncthreads();
 
-    // Per-digit warp offsets, tile counts, and the look-back over the
-    // segment's earlier tiles.
+    // Per-digit warp offsets and tile counts; the tile's counts are published
+    // at once so later tiles can look back past it.
+    const uint32_t dg_me = threadIdx.x;  // SORT_BLOCK == 256: one digit per thread
+    uint32_t run = 0;
     {
-        const uint32_t dg = threadIdx.x;  // SORT_BLOCK == 256
-        uint32_t run = 0;
 #pragma unroll
         for (int ww = 0; ww < NW; ++ww) {
-            const uint32_t c = warp_hist[ww][dg];
-            warp_hist[ww][dg] = run;
+            const uint32_t c = warp_hist[ww][dg_me];
+            warp_hist[ww][dg_me] = run;
             run += c;
         }
-        uint32_t* my = lb + (uint64_t)item * 256 + dg;
-        uint32_t excl = 0;
-        if (tile == 0) {
-            st_volatile_u32(my, LB_INC | run);
-        } else {
-            st_volatile_u32(my, LB_AGG | run);
-            int64_t t = (int64_t)item - 1;
-            const int64_t t_end = (int64_t)d.item_begin;
-            uint32_t spins = 0;
-            while (t >= t_end) {
-                const uint32_t v = ld_volatile_u32(lb + (uint64_t)t * 256 + dg);
-                const uint32_t st = v >> 30;
-                if (st == 0) {
-                    if (++spins > LB_SPIN_LIMIT) {
-                        atomicOr(a.status, ST_FLAG_TIMEOUT);
-                        break;
-                    }
-                    if (spins > 4) __nanosleep(64);
-                    continue;
-                }
-                excl += v & LB_VAL;
-                if (st == 2) break;
-                --t;
-            }
-            st_volatile_u32(my, LB_INC | ((excl + run) & LB_VAL));
-        }
-        lb_next[(uint64_t)item * 256 + dg] = 0;
-        gstart[dg] = a.digit_base[((uint64_t)sg * KeyTraits<K>::NPASS + p) * 256 + dg] + excl;
+        st_volatile_u32(lb + (uint64_t)item * 256 + dg_me, (tile == 0 ? LB_INC : LB_AGG) | run);
         // Exclusive scan of the tile's digit counts.
         uint32_t x = run;
 #pragma unroll
@@ -321,33 +298,80 @@ __global__ void __launch_bounds__(SORT_BLOCK) sort_pass_kernel(SortArgs a, int p
         __syncthreads();
         uint32_t wp = 0;
         for (int i = 0; i < w; ++i) wp += wsum[i];
-        tile_off[dg] = wp + x - run;
+        tile_off[dg_me] = wp + x - run;
     }
     __syncthreads();
 
-    // Stage digit-sorted, then write coalesced runs.
+    // Stage the tile digit-sorted (keys unless this is the last pass,
+    // payloads, digits); the registers are free for the look-back.
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
         const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
         if (e < n) {
             const uint32_t dg = (uint32_t)(key[j] >> shift) & 0xFFu;
             const uint32_t pos = tile_off[dg] + warp_hist[w][dg] + rank[j];
-            stage_key[pos] = key[j];
+            stage_dig[pos] = (uint8_t)dg;
+            if (kout) stage_key[pos] = key[j];
             stage_pay[pos] = pay[j];
         }
     }
+
+    // Look back over the segment's earlier tiles, LB_WINDOW words in flight
+    // at a time: sum aggregates until an inclusive prefix.
+    {
+        uint32_t excl = 0;
+        if (tile != 0) {
+            int64_t t = (int64_t)item - 1;
+            const int64_t t_end = (int64_t)d.item_begin;
+            uint32_t spins = 0;
+            while (t >= t_end) {
+                const int cnt = (t - t_end + 1) < LB_WINDOW ? (int)(t - t_end + 1) : LB_WINDOW;
+                uint32_t v[LB_WINDOW];
+#pragma unroll
+                for (int i = 0; i < LB_WINDOW; ++i)
+                    v[i] = i < cnt ? ld_volatile_u32(lb + (uint64_t)(t - i) * 256 + dg_me) : 0u;
+                int used = 0;
+                bool done = false, stalled = false;
+#pragma unroll
+                for (int i = 0; i < LB_WINDOW; ++i) {
+                    if (done || stalled || i >= cnt) continue;
+                    const uint32_t st = v[i] >> 30;
+                    if (st == 0) {
+                        stalled = true;  // not published yet: poll again from here
+                        continue;
+                    }
+                    excl += v[i] & LB_VAL;
+                    ++used;
+                    if (st == 2) done = true;
+                }
+                if (done) break;
+                t -= used;
+                if (stalled) {
+                    if (++spins > LB_SPIN_LIMIT) {
+                        atomicOr(a.status, ST_FLAG_TIMEOUT);
+                        break;
+                    }
+                    if (spins > 4) __nanosleep(64);
+                }
+            }
+            st_volatile_u32(lb + (uint64_t)item * 256 + dg_me, LB_INC | ((excl + run) & LB_VAL));
+        }
+        lb_next[(uint64_t)item * 256 + dg_me] = 0;
+        gstart[dg_me] = a.digit_base[((uint64_t)sg * KeyTraits<K>::NPASS + p) * 256 + dg_me] + excl;
+    }
     __syncthreads();
+
+    // Coalesced runs out of the staged tile.
     const uint64_t tb = (uint64_t)tile * SORT_TILE;
     const uint32_t tile_n = (uint32_t)((n - tb) < (uint64_t)SORT_TILE ? (n - tb) : (uint64_t)SORT_TILE);
     for (uint32_t i = threadIdx.x; i < tile_n; i += SORT_BLOCK) {
-        const K k = stage_key[i];
-        const uint32_t dg = (uint32_t)(k >> shift) & 0xFFu;
+        const uint32_t dg = stage_dig[i];
         const uint64_t g = (uint64_t)gstart[dg] + (i - tile_off[dg]);
         if (g >= n) {  // only reachable after a look-back timeout
             atomicOr(a.status, ST_FLAG_TIMEOUT);
             continue;
         }
-        if (kout) kout[g] = k;
+        if (kout) kout[g] = stage_key[i];
         pout[g] = stage_pay[i];
     }
 }
@@ -413,7 +437,7 @@ bolt_status run_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
     sort_hist_kernel<K><<<hb, 256, 0, s>>>(a);
     sort_scan_kernel<NP><<<nseg, 256, 0, s>>>(a);
     ctx->last_launches += 2;
-    const size_t dyn = (sizeof(K) + 4) * SORT_TILE;
+    const size_t dyn = (sizeof(K) + 5) * SORT_TILE;
     BOLT_CUDA(ctx, cudaFuncSetAttribute(sort_pass_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     for (int p = 0; p < NP; ++p) {
         sort_pass_kernel<K><<<(unsigned)items, SORT_BLOCK, dyn, s>>>(a, p);
