@@ -263,8 +263,7 @@ bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& sp
         if (spec.col[c].out_valid) BOLT_CUDA(ctx, cudaMemsetAsync(spec.col[c].out_valid, 0, (rows + 7) / 8, s));
     }
     if (staged) {
-        BOLT_CUDA(ctx, cudaFuncSetAttribute(compact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)stage_bytes));
+        BOLT_CUDA(ctx, smem_optin(compact_kernel<true>, ctx));
         compact_kernel<true><<<(unsigned)ntiles, CP_BLOCK, stage_bytes, s>>>(a);
     } else {
         compact_kernel<false><<<(unsigned)ntiles, CP_BLOCK, 0, s>>>(a);

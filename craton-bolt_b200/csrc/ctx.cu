@@ -1,6 +1,10 @@
 // ctx.cu — context lifecycle, arena, status plumbing and small ABI helpers.
 #include "ctx.cuh"
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include <cstring>
 
 namespace bolt {
@@ -82,6 +86,21 @@ bolt_status call_end(bolt_ctx* ctx, uint32_t flags, cudaStream_t s) {
     }
     if (flags & BOLT_FLAG_ASYNC) ctx->async_pending++;
     return BOLT_OK;
+}
+
+cudaError_t ensure_smem_optin(const void* kernel, int device, int max_optin) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({kernel, device})) return cudaSuccess;
+    // The limit covers dynamic memory only: leave room for the static part.
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    const int dyn = max_optin - (int)fa.sharedSizeBytes;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn > 0 ? dyn : 0);
+    if (e == cudaSuccess) done.insert({kernel, device});
+    return e;
 }
 
 bolt_status read_status(bolt_ctx* ctx, cudaStream_t s, int n_words, uint32_t* flags) {

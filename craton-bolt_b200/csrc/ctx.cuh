@@ -73,6 +73,16 @@ bolt_status cuda_fail(bolt_ctx* ctx, cudaError_t e, const char* where);
         if (_e != cudaSuccess) return bolt::cuda_fail(ctx, _e, #call); \
     } while (0)
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum, once per (kernel, device). The attribute is process-wide, so
+// per-call values would race between host threads that launch the same
+// kernel with different sizes; one maximal value never does.
+cudaError_t ensure_smem_optin(const void* kernel, int device, int max_optin);
+template <class F>
+inline cudaError_t smem_optin(F* kernel, const bolt_ctx* ctx) {
+    return ensure_smem_optin(reinterpret_cast<const void*>(kernel), ctx->device, ctx->max_smem_optin);
+}
+
 // Arena allocation (256-byte aligned); returns nullptr when exhausted.
 void* arena_alloc(bolt_ctx* ctx, uint64_t bytes);
 inline void arena_reset(bolt_ctx* ctx) { ctx->arena_used = ctx->arena_pinned; }

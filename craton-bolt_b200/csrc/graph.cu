@@ -82,7 +82,7 @@ extern "C" bolt_status bolt_batch_graph_create(int device, bolt_query* qs, int32
         return BOLT_ERR_CUDA;
     }
     cudaMemsetAsync(ctx->d_status, 0, 16, g->cap_stream);
-    st = gb_run(ctx, run.data(), n, g->cap_stream, 0);
+    st = gb_run(ctx, run.data(), n, g->cap_stream, 0, true);
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(g->cap_stream, &graph);
     if (st != BOLT_OK || ce != cudaSuccess) {

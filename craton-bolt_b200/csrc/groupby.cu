@@ -1545,7 +1545,7 @@ namespace {
 bolt_status launch_batch_agg(bolt_ctx* ctx, cudaStream_t s, BatchKernel kfn, const GbParams* d_prms,
                              const uint32_t* d_begins, int nq, uint32_t items, uint32_t item_tiles, uint32_t* counter,
                              size_t smem, int block) {
-    BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BOLT_CUDA(ctx, smem_optin(kfn, ctx));
     int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
@@ -1592,7 +1592,7 @@ bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& pl, GbStagedLaunch* out
 }
 
 // Allocates and zeroes the queries' tables and words and points the plans at them.
-static bolt_status gb_run_tables(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s) {
+static bolt_status gb_run_tables(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, bool query_status) {
     if (nq <= 0) return BOLT_OK;
     // Tables and per-query words (occupancy, groups, status) in one zeroed region.
     std::vector<uint64_t> toff(nq);
@@ -1615,8 +1615,9 @@ static bolt_status gb_run_tables(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream
         p.gtab = (ull*)(region + toff[q]);
         p.occupancy = w;
         // A single query reports through the context's status word (so
-        // bolt_ctx_sync_status sees it); batched queries each get their own.
-        p.status = nq == 1 ? ctx->d_status : (uint32_t*)(w + 3);
+        // bolt_ctx_sync_status sees it); batched queries each get their own,
+        // also in a batch of one.
+        p.status = (nq == 1 && !query_status) ? ctx->d_status : (uint32_t*)(w + 3);
         f.gtab = p.gtab;
         f.n_nonnull = w + 1;
         f.n_groups = w + 2;
@@ -1660,7 +1661,7 @@ static bolt_status gb_agg_one(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_
         tiles = (p.n_rows + tile - 1) / tile;
     }
     int per_sm = 1;
-    BOLT_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BOLT_CUDA(ctx, smem_optin(kfn, ctx));
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, std::max<uint64_t>(tiles, 1));
@@ -1669,6 +1670,7 @@ static bolt_status gb_agg_one(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_
     if (p.n_rows > 0) {
         kernel_mark_begin(ctx, flags, s);
         kfn<<<pl->grid, block, smem, s>>>(p);
+        BOLT_CUDA(ctx, cudaGetLastError());
         ctx->last_launches++;
         kernel_mark_end(ctx, flags, s);
     }
@@ -1765,7 +1767,7 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
         bolt_status st = stage_upload(ctx, s, d_f, small.data(), sizeof(GbFinal) * small.size());
         if (st != BOLT_OK) return st;
         const size_t fsm = (size_t)small_cap * 2 * 12;
-        BOLT_CUDA(ctx, cudaFuncSetAttribute(gb_small_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+        BOLT_CUDA(ctx, smem_optin(gb_small_final_kernel, ctx));
         gb_small_final_kernel<<<(unsigned)small.size(), 1024, fsm, s>>>(d_f);
         ctx->last_launches++;
     }
@@ -1814,9 +1816,9 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
     return BOLT_OK;
 }
 
-bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags) {
+bolt_status gb_run(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_t s, uint32_t flags, bool query_status) {
     if (nq <= 0) return BOLT_OK;
-    bolt_status st = gb_run_tables(ctx, pls, nq, s);
+    bolt_status st = gb_run_tables(ctx, pls, nq, s, query_status);
     if (st == BOLT_OK) st = gb_run_aggregate(ctx, pls, nq, s, flags);
     if (st == BOLT_OK) st = gb_run_finalize(ctx, pls, nq, s);
     return st;
@@ -1828,10 +1830,13 @@ using namespace bolt;
 
 extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64_t n_rows) {
     if (!desc) return 0;
-    // Table words per slot: key + up to two words per aggregate state.
-    const uint64_t words = 1 + 2ull * (uint64_t)(desc->n_aggs > 0 ? desc->n_aggs : 1);
-    const uint64_t groups = desc->groups_hint ? desc->groups_hint : std::min<uint64_t>(n_rows, 1ull << 15);
-    const uint64_t cap = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * groups + 16, 64));
+    // Table words per slot: key + at most three words per aggregate (AVG: a
+    // two-word sum and a count); slots as the planner sizes them untuned
+    // (4x the expected groups, or 2x the rows up to 64K without a hint).
+    const uint64_t words = 1 + 3ull * (uint64_t)(desc->n_aggs > 0 ? desc->n_aggs : 1);
+    const uint64_t want = desc->groups_hint ? (desc->groups_hint << 2) + 16
+                                            : std::min<uint64_t>(2 * n_rows + 16, 1ull << 16);
+    const uint64_t cap = 1ull << ceil_log2_u64(std::max<uint64_t>(want, 64));
     uint64_t bytes = (cap + 2) * words * 8 + 4096;
     if (cap > 8192) bytes += (cap + 1) * 16 + radix_sort_scratch(cap + 1, 1, SRC_U64_KEYS);
     return bytes;
@@ -2041,7 +2046,7 @@ static bolt_status gb_host(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_group
         if (st != BOLT_OK) return st;
         pl.fin.n_groups_user = nullptr;
         GbPlan* one = &pl;
-        st = gb_run_tables(ctx, &one, 1, s);
+        st = gb_run_tables(ctx, &one, 1, s, false);
         if (st != BOLT_OK) return st;
         const GbParams base = pl.prm;
         // The ring may still be read by an earlier call's kernels on `s`.
@@ -2236,15 +2241,14 @@ extern "C" bolt_status bolt_groupby_noalloc(const bolt_groupby_desc* desc, bolt_
         const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)c.num_sms, std::max<uint64_t>(tiles, 1));
         if (p.n_rows > 0) {
             const AggKernel kfn = agg_kernel_for(p.spec, p.n_st);
-            if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            if (smem_optin(kfn, &c) != cudaSuccess)
                 return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: shared-memory attribute failed");
             kfn<<<grid, pl.block, smem, s>>>(p);
             if (cudaGetLastError() != cudaSuccess)
                 return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: aggregation launch failed");
         }
         const size_t fsm = (size_t)pl.cap * 2 * 12;
-        if (cudaFuncSetAttribute(gb_small_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) !=
-            cudaSuccess)
+        if (smem_optin(gb_small_final_kernel, &c) != cudaSuccess)
             return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: shared-memory attribute failed");
         gb_small_final_kernel<<<1, 1024, fsm, s>>>(d_final);
         if (cudaGetLastError() != cudaSuccess) return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: finalize launch failed");
@@ -2339,7 +2343,21 @@ extern "C" bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* qs, int32_t
         run.push_back(&plans[i]);
         idx.push_back(i);
     }
-    st = gb_run(ctx, run.data(), (int)run.size(), s, flags);
+    st = gb_run(ctx, run.data(), (int)run.size(), s, flags, true);
+    if (st == BOLT_ERR_CAPACITY && run.size() > 1 && !(flags & BOLT_FLAG_ASYNC)) {
+        // The batch's tables do not fit the arena together: run each query
+        // alone (each call starts from an empty arena).
+        BOLT_CUDA(ctx, cudaStreamSynchronize(s));
+        ctx->last_error.clear();
+        for (int i : idx)
+            qs[i].status = gb_single(ctx, &qs[i].desc, &qs[i].out, qs[i].row_begin, qs[i].row_end,
+                                     flags & ~BOLT_FLAG_PROFILE, s, nullptr, nullptr, "batched GROUP BY");
+        for (int i = 0; i < n; ++i)
+            if (qs[i].status != BOLT_OK)
+                return fail(ctx, qs[i].status, "batched GROUP BY: query %d failed (%s)", i,
+                            bolt_status_str(qs[i].status));
+        return BOLT_OK;
+    }
     if (st != BOLT_OK) return st;
     st = call_end(ctx, flags, s);
     if (st != BOLT_OK) return st;
@@ -2356,12 +2374,17 @@ extern "C" bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* qs, int32_t
         bolt_query& q = qs[idx[j]];
         const uint32_t f = (uint32_t)w[(size_t)j * 8 + 3];
         q.out.n_groups = w[(size_t)j * 8 + 2];
-        if (f & (ST_FLAG_GROW | ST_FLAG_SPILL | ST_FLAG_RANGE | ST_FLAG_DECRANGE)) {
+        // Re-run alone: a bigger table or another accumulator mode, or a
+        // SUM(Int64) whose row-order prefixes need the exact check.
+        const bool i64_check = run[j]->prm.i64_bits &&
+                               (uint32_t)w[(size_t)j * 8 + 4] + (uint32_t)ceil_log2_u64(run[j]->prm.n_rows + 1) >= 63;
+        if ((f & (ST_FLAG_GROW | ST_FLAG_SPILL | ST_FLAG_RANGE | ST_FLAG_DECRANGE)) || (f == 0 && i64_check)) {
             redo.push_back(idx[j]);
             continue;
         }
         if (f & ST_FLAG_DECOVERFLOW) q.status = BOLT_ERR_OVERFLOW;
         else if (f & ST_FLAG_OVERFLOW) q.status = BOLT_ERR_OVERFLOW;
+        else if (f & ST_FLAG_TIMEOUT) q.status = BOLT_ERR_TIMEOUT;
         else if (f & ST_FLAG_CAPACITY) q.status = BOLT_ERR_CAPACITY;
         else q.status = BOLT_OK;
     }

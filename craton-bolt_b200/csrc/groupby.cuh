@@ -184,6 +184,8 @@ bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& plan, GbStagedLaunch* o
 
 // Allocates scratch and enqueues table init, aggregation and finalize of
 // `nq` planned queries (one persistent aggregation launch when nq > 1).
-bolt_status gb_run(bolt_ctx* ctx, GbPlan** plans, int nq, cudaStream_t s, uint32_t flags);
+// query_status: every query reports through its own status word (batches),
+// even when nq == 1; otherwise a single query reports through the context's.
+bolt_status gb_run(bolt_ctx* ctx, GbPlan** plans, int nq, cudaStream_t s, uint32_t flags, bool query_status = false);
 
 }  // namespace bolt

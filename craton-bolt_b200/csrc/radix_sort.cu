@@ -438,7 +438,7 @@ bolt_status run_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
     sort_scan_kernel<NP><<<nseg, 256, 0, s>>>(a);
     ctx->last_launches += 2;
     const size_t dyn = (sizeof(K) + 5) * SORT_TILE;
-    BOLT_CUDA(ctx, cudaFuncSetAttribute(sort_pass_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    BOLT_CUDA(ctx, smem_optin(sort_pass_kernel<K>, ctx));
     for (int p = 0; p < NP; ++p) {
         sort_pass_kernel<K><<<(unsigned)items, SORT_BLOCK, dyn, s>>>(a, p);
         ctx->last_launches++;

@@ -4,9 +4,10 @@
 // one synchronous stream (src/exec/launch.rs:308-368). Here:
 //   * `n_lanes` worker threads, each owning a bolt_ctx (scratch arena) and a
 //     CUDA stream, so batches on different lanes overlap on the device;
-//   * a FIFO queue of submitted queries; an idle lane admits queries from
-//     the head while their summed HBM footprint (bolt_groupby_footprint)
-//     fits its share of the budget and the batch is below `max_batch`;
+//   * a queue of submitted queries; an idle lane admits a large query at
+//     the head alone, else small queries in arrival order while their summed
+//     HBM footprint (bolt_groupby_footprint) fits its share of the budget and
+//     the batch is below `max_batch`;
 //   * the lane runs its batch as one bolt_batch_groupby call (one persistent
 //     aggregation launch + one batched finalize) and completes the tickets;
 //   * queries that arrive while lanes are busy wait only until some lane
@@ -56,6 +57,9 @@ namespace {
 
 uint64_t query_rows(const bolt_query* q) { return q->row_end > q->row_begin ? q->row_end - q->row_begin : 0; }
 
+// Queries with at least this many rows are admitted alone.
+constexpr uint64_t BIG_QUERY_ROWS = 4ull << 20;
+
 void lane_loop(bolt_server* srv, int lane) {
     cudaSetDevice(srv->cfg.device);
     bolt_ctx* ctx = srv->ctx[lane];
@@ -68,14 +72,32 @@ void lane_loop(bolt_server* srv, int lane) {
             std::unique_lock<std::mutex> lk(srv->mu);
             srv->cv_work.wait(lk, [&] { return srv->stop || !srv->queue.empty(); });
             if (srv->stop && srv->queue.empty()) return;
-            // Admission: FIFO while the summed footprint fits the lane's share.
-            uint64_t used = 0;
-            while (!srv->queue.empty() && (int)batch.size() < srv->cfg.max_batch) {
-                Req* r = srv->queue.front();
-                if (!batch.empty() && used + r->footprint > srv->lane_budget) break;
+            // Admission. A large query at the head runs as a batch of its own;
+            // otherwise the lane takes small queries in arrival order (passing
+            // over large ones, which stay queued for the next free lane)
+            // while the summed footprint fits the lane's share, so small
+            // queries never wait behind a large one inside a batch.
+            Req* head = srv->queue.front();
+            if (query_rows(head->q) >= BIG_QUERY_ROWS) {
                 srv->queue.pop_front();
-                used += r->footprint;
-                batch.push_back(r);
+                batch.push_back(head);
+            } else {
+                uint64_t used = 0;
+                std::deque<Req*> rest;
+                while (!srv->queue.empty()) {
+                    Req* r = srv->queue.front();
+                    srv->queue.pop_front();
+                    const bool take = query_rows(r->q) < BIG_QUERY_ROWS &&
+                                      (int)batch.size() < srv->cfg.max_batch &&
+                                      (batch.empty() || used + r->footprint <= srv->lane_budget);
+                    if (take) {
+                        used += r->footprint;
+                        batch.push_back(r);
+                    } else {
+                        rest.push_back(r);
+                    }
+                }
+                srv->queue.swap(rest);
             }
         }
         if (!srv->queue.empty()) srv->cv_work.notify_one();

@@ -141,12 +141,15 @@ def test_batch_graph_replay(bolt, engine, oracle):
         g.close()
 
 
-def test_server_mix_equals_alone(bolt, engine, oracle):
-    n = 300_000
+@pytest.mark.parametrize("n,n_q,lanes", [(300_000, 60, 2), (12_000_000, 24, 4)])
+def test_server_mix_equals_alone(bolt, engine, oracle, n, n_q, lanes):
+    """Served results equal the query run alone. The larger table gives
+    queries above the size that is admitted alone, and four lanes run
+    different kernels and shared-memory sizes concurrently."""
     t, dts, dev = make_table(bolt, n, 5)
-    specs = query_specs(n, 60, 6)
+    specs = query_specs(n, n_q, 6)
     kdev, khost = keyed_columns(bolt, t, dts, specs)
-    srv = bolt.Server(0, scratch_bytes=2 << 30, max_batch=16, n_lanes=2)
+    srv = bolt.Server(0, scratch_bytes=4 << 30, max_batch=16, n_lanes=lanes)
     try:
         tickets = []
         for s in specs:
