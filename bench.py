@@ -687,6 +687,23 @@ def w_batch(c: Ctx):
             lat_poisson = [srv.wait(t)[1] for t in tickets]
         finally:
             srv.close()
+        # The same Poisson arrivals served one query at a time (FIFO): latency
+        # from arrival to completion.
+        prepared4 = [prep(q, sliced=True) for q in qs]
+        torch.cuda.synchronize()
+        lat_single_poisson = []
+        t0 = time.perf_counter()
+        arrive = t0
+        for pq, gap in zip(prepared4, gaps):
+            arrive += gap
+            while time.perf_counter() < arrive:
+                pass
+            st = c.lib.bolt_groupby(c.eng._ctx, C.byref(pq.desc), C.byref(pq.out), 0,
+                                    C.c_void_p(c.stream.cuda_stream))
+            if st != 0:
+                raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+            lat_single_poisson.append((time.perf_counter() - arrive) * 1e6)
+        del prepared4
         return {"queries": len(qs), "rows_total": total_rows, "batched_qps": batch_qps,
                 "one_at_a_time_qps": single_qps, "speedup": batch_qps / single_qps,
                 "rows_per_s_batched": total_rows / batch_s, "batch_s": batch_s,
@@ -695,6 +712,8 @@ def w_batch(c: Ctx):
                                "one_at_a_time_p99": float(np.percentile(lat_single, 99)),
                                "served_poisson_p50": float(np.percentile(lat_poisson, 50)),
                                "served_poisson_p99": float(np.percentile(lat_poisson, 99)),
+                               "one_at_a_time_poisson_p50": float(np.percentile(lat_single_poisson, 50)),
+                               "one_at_a_time_poisson_p99": float(np.percentile(lat_single_poisson, 99)),
                                "poisson_rate_qps": rate}}
 
     main_mix = measure(batch_queries(a.batch_queries, n))
@@ -781,7 +800,7 @@ def main():
     ap.add_argument("--batch-queries", type=int, default=4096)
     ap.add_argument("--batch-table-rows", type=int, default=50_000_000)
     ap.add_argument("--max-batch", type=int, default=512)
-    ap.add_argument("--lanes", type=int, default=2)
+    ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--server-scratch-gb", type=int, default=64)
     ap.add_argument("--scratch-gb", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -1133,6 +1133,11 @@ __global__ void __launch_bounds__(256) gb_prefix_check_kernel(const __grid_const
     }
 }
 
+// Items one CTA of the multi-query kernel takes before it exits: CTAs of
+// bounded length (about 130K rows) let the scheduler interleave other
+// streams' higher-priority blocks between them.
+constexpr uint32_t BATCH_CTA_ITEMS = 16;
+
 // Persistent multi-query aggregation: work items are (query, run of
 // item_tiles tiles of blockDim.x * U rows) handed out in order from one
 // counter. A CTA keeps one query's shared table while its items stay on that
@@ -1150,7 +1155,7 @@ __global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_batch_agg_kernel(
     int cur = -1, stopped = -1;
     int C = 0;
     uint32_t inserts = 0, pending = 0, absbits = 0;
-    for (uint32_t it = 0;; ++it) {
+    for (uint32_t it = 0; it < BATCH_CTA_ITEMS; ++it) {
         if (threadIdx.x == 0) s_item[it & 1] = atomicAdd(counter, 1u);
         __syncthreads();
         const uint32_t item = s_item[it & 1];
@@ -1549,7 +1554,11 @@ bolt_status launch_batch_agg(bolt_ctx* ctx, cudaStream_t s, BatchKernel kfn, con
     int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, block, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
-    const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, items);
+    // Enough CTAs for every item at BATCH_CTA_ITEMS each, and at least a
+    // full wave.
+    const uint64_t need = ((uint64_t)items + BATCH_CTA_ITEMS - 1) / BATCH_CTA_ITEMS;
+    const unsigned grid =
+        (unsigned)std::max<uint64_t>(need, std::min<uint64_t>((uint64_t)per_sm * ctx->num_sms, items));
     kfn<<<grid, block, smem, s>>>(d_prms, d_begins, nq, items, item_tiles, counter);
     ctx->last_launches++;
     return BOLT_OK;

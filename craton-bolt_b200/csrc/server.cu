@@ -6,14 +6,16 @@
 //     CUDA stream, so batches on different lanes overlap on the device;
 //   * a queue of submitted queries; an idle lane admits a large query at
 //     the head alone, else small queries in arrival order while their summed
-//     HBM footprint (bolt_groupby_footprint) fits its share of the budget and
-//     the batch is below `max_batch`;
+//     HBM footprint (bolt_groupby_footprint) fits its share of the budget,
+//     their summed rows stay below a work cap and the batch is below
+//     `max_batch`;
 //   * the lane runs its batch as one bolt_batch_groupby call (one persistent
 //     aggregation launch + one batched finalize) and completes the tickets;
 //   * queries that arrive while lanes are busy wait only until some lane
 //     frees, then join the next batch (continuous batching).
 // Results are identical alone or in any mix: every accumulator is order-
 // independent (integer states, fixed-point float sums).
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -50,6 +52,7 @@ struct bolt_server {
     std::unordered_map<uint64_t, Req*> reqs;
     uint64_t next_ticket = 1;
     uint64_t lane_budget = 0;
+    uint64_t n_big = 0;  // queued queries of at least BIG_QUERY_ROWS rows
     bool stop = false;
 };
 
@@ -57,8 +60,11 @@ namespace {
 
 uint64_t query_rows(const bolt_query* q) { return q->row_end > q->row_begin ? q->row_end - q->row_begin : 0; }
 
-// Queries with at least this many rows are admitted alone.
+// Queries with at least this many rows are admitted alone, and a batch of
+// smaller ones holds at most BATCH_ROWS_MAX rows (a few milliseconds of
+// device work), which bounds how long a query waits for its batch.
 constexpr uint64_t BIG_QUERY_ROWS = 4ull << 20;
+constexpr uint64_t BATCH_ROWS_MAX = 32ull << 20;
 
 void lane_loop(bolt_server* srv, int lane) {
     cudaSetDevice(srv->cfg.device);
@@ -69,29 +75,46 @@ void lane_loop(bolt_server* srv, int lane) {
     for (;;) {
         batch.clear();
         {
+            // The first half of the lanes serve the large queries (at most
+            // that many run at once, so they do not all stretch each other's
+            // tail latency) and small ones when none is queued; the other
+            // lanes serve only small queries. With one lane it goes by arrival.
+            const bool big_lane = lane < std::max(1, srv->cfg.n_lanes / 2);
+            const bool solo = srv->cfg.n_lanes == 1;
             std::unique_lock<std::mutex> lk(srv->mu);
-            srv->cv_work.wait(lk, [&] { return srv->stop || !srv->queue.empty(); });
-            if (srv->stop && srv->queue.empty()) return;
-            // Admission. A large query at the head runs as a batch of its own;
-            // otherwise the lane takes small queries in arrival order (passing
-            // over large ones, which stay queued for the next free lane)
-            // while the summed footprint fits the lane's share, so small
-            // queries never wait behind a large one inside a batch.
-            Req* head = srv->queue.front();
-            if (query_rows(head->q) >= BIG_QUERY_ROWS) {
-                srv->queue.pop_front();
-                batch.push_back(head);
+            srv->cv_work.wait(lk, [&] {
+                return srv->stop || (big_lane ? !srv->queue.empty() : srv->queue.size() > srv->n_big);
+            });
+            if (big_lane ? srv->queue.empty() : srv->queue.size() <= srv->n_big) return;  // stopping
+            Req* big = nullptr;
+            if (big_lane && srv->n_big > 0 &&
+                (!solo || query_rows(srv->queue.front()->q) >= BIG_QUERY_ROWS)) {
+                for (auto it = srv->queue.begin(); it != srv->queue.end(); ++it)
+                    if (query_rows((*it)->q) >= BIG_QUERY_ROWS) {
+                        big = *it;
+                        srv->queue.erase(it);
+                        --srv->n_big;
+                        break;
+                    }
+            }
+            if (big) {
+                batch.push_back(big);
             } else {
-                uint64_t used = 0;
+                // Small queries in arrival order (passing over large ones),
+                // while the summed footprint fits the lane's share and the
+                // summed rows the work cap.
+                uint64_t used = 0, rows = 0;
                 std::deque<Req*> rest;
                 while (!srv->queue.empty()) {
                     Req* r = srv->queue.front();
                     srv->queue.pop_front();
-                    const bool take = query_rows(r->q) < BIG_QUERY_ROWS &&
-                                      (int)batch.size() < srv->cfg.max_batch &&
-                                      (batch.empty() || used + r->footprint <= srv->lane_budget);
+                    const uint64_t qr = query_rows(r->q);
+                    const bool take = qr < BIG_QUERY_ROWS && (int)batch.size() < srv->cfg.max_batch &&
+                                      (batch.empty() || (used + r->footprint <= srv->lane_budget &&
+                                                         rows + qr <= BATCH_ROWS_MAX));
                     if (take) {
                         used += r->footprint;
+                        rows += qr;
                         batch.push_back(r);
                     } else {
                         rest.push_back(r);
@@ -100,7 +123,7 @@ void lane_loop(bolt_server* srv, int lane) {
                 srv->queue.swap(rest);
             }
         }
-        if (!srv->queue.empty()) srv->cv_work.notify_one();
+        if (!srv->queue.empty()) srv->cv_work.notify_all();
         qs.resize(batch.size());
         for (size_t i = 0; i < batch.size(); ++i) qs[i] = *batch[i]->q;
         const bolt_status st = bolt_batch_groupby(ctx, qs.data(), (int32_t)qs.size(), 0, (bolt_stream)s);
@@ -147,7 +170,13 @@ extern "C" bolt_status bolt_server_create(const bolt_server_config* cfg, bolt_se
         bolt_ctx* c = nullptr;
         bolt_status st = bolt_ctx_create(cfg->device, per_lane, &c);
         cudaStream_t s = nullptr;
-        if (st != BOLT_OK || cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        // The large-query lanes get the highest stream priority: their
+        // blocks are scheduled first as SMs free up, so a large query runs
+        // at close to its solo speed while the small batches fill in.
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        const int prio = (i < std::max(1, srv->cfg.n_lanes / 2) && srv->cfg.n_lanes > 1) ? hi : lo;
+        if (st != BOLT_OK || cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio) != cudaSuccess) {
             if (c) bolt_ctx_destroy(c);
             bolt_server_destroy(srv);
             return st != BOLT_OK ? st : BOLT_ERR_CUDA;
@@ -175,9 +204,10 @@ extern "C" bolt_status bolt_server_submit(bolt_server* srv, bolt_query* q, uint6
         r->ticket = srv->next_ticket++;
         srv->reqs[r->ticket] = r;
         srv->queue.push_back(r);
+        if (query_rows(q) >= BIG_QUERY_ROWS) ++srv->n_big;
     }
     *ticket = r->ticket;
-    srv->cv_work.notify_one();
+    srv->cv_work.notify_all();
     return BOLT_OK;
 }
 
