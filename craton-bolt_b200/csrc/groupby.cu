@@ -932,7 +932,14 @@ constexpr int FIN_CHUNK = 4096;
 // (query, chunk of 4096 slots); order key = packed key ^ sign bit.
 __global__ void __launch_bounds__(256) gb_compact_batch_kernel(const GbFinal* fins, const uint32_t* begins, int nq,
                                                                 uint32_t total_items) {
+    // Each warp takes runs of 32 x CMP_ROUNDS slots: it reads their keys,
+    // counts the occupied ones with ballots, claims that many output rows
+    // with one atomic, then writes them (one atomic per 512 slots instead of
+    // per 32 keeps the shared counter out of the way).
+    constexpr int CMP_ROUNDS = 16;
     __shared__ __align__(16) GbFinal f;
+    const uint32_t lane = lane_id();
+    const int warp = (int)(threadIdx.x >> 5), nwarps = (int)(blockDim.x >> 5);
     for (uint32_t item = blockIdx.x; item < total_items; item += gridDim.x) {
         const int q = query_of(begins, nq, item);
         __syncthreads();
@@ -940,27 +947,42 @@ __global__ void __launch_bounds__(256) gb_compact_batch_kernel(const GbFinal* fi
         const ull cap = 1ull << f.log2cap;
         const uint64_t c0 = (uint64_t)(item - begins[q]) * FIN_CHUNK;
         const uint64_t c1 = c0 + FIN_CHUNK < cap + 1 ? c0 + FIN_CHUNK : cap + 1;
-        for (uint64_t base = c0; base < c1; base += blockDim.x) {
-            const uint64_t i = base + threadIdx.x;
-            bool occ = false;
-            ull ok = 0;
-            if (i < cap) {
-                const ull k = ld_volatile(f.gtab + i * (ull)f.slot_words);
-                occ = k != 0;
-                ok = ~k ^ 0x8000000000000000ull;
-            } else if (i == cap) {
-                occ = f.gtab[cap * (ull)f.slot_words] != 0;
-                ok = ~0ull ^ 0x8000000000000000ull;
+        for (uint64_t run = c0 + (uint64_t)warp * 32 * CMP_ROUNDS; run < c1;
+             run += (uint64_t)nwarps * 32 * CMP_ROUNDS) {
+            ull ok[CMP_ROUNDS];
+            uint32_t occ = 0, total = 0;
+#pragma unroll
+            for (int j = 0; j < CMP_ROUNDS; ++j) {
+                const uint64_t i = run + (uint64_t)j * 32 + lane;
+                bool o = false;
+                ok[j] = 0;
+                if (i < c1) {
+                    if (i < cap) {
+                        const ull k = ld_volatile(f.gtab + i * (ull)f.slot_words);
+                        o = k != 0;
+                        ok[j] = ~k ^ 0x8000000000000000ull;
+                    } else {  // i == cap: the key whose complement is 0
+                        o = f.gtab[cap * (ull)f.slot_words] != 0;
+                        ok[j] = ~0ull ^ 0x8000000000000000ull;
+                    }
+                }
+                total += __popc(__ballot_sync(0xffffffffu, o));
+                if (o) occ |= 1u << j;
             }
-            const uint32_t m = __ballot_sync(0xffffffffu, occ);
-            if (!m) continue;
+            if (!total) continue;
             ull pos = 0;
-            if (lane_id() == (uint32_t)(__ffs(m) - 1)) pos = atomicAdd(f.n_nonnull, (ull)__popc(m));
-            pos = __shfl_sync(0xffffffffu, pos, __ffs(m) - 1);
-            if (occ) {
-                pos += __popc(m & lanemask_lt());
-                f.order_keys[pos] = ok;
-                f.slots[pos] = (uint32_t)i;
+            if (lane == 0) pos = atomicAdd(f.n_nonnull, (ull)total);
+            pos = __shfl_sync(0xffffffffu, pos, 0);
+#pragma unroll
+            for (int j = 0; j < CMP_ROUNDS; ++j) {
+                const bool o = (occ >> j) & 1u;
+                const uint32_t m = __ballot_sync(0xffffffffu, o);
+                if (o) {
+                    const ull at = pos + __popc(m & lanemask_lt());
+                    f.order_keys[at] = ok[j];
+                    f.slots[at] = (uint32_t)(run + (uint64_t)j * 32 + lane);
+                }
+                pos += __popc(m);
             }
         }
     }
@@ -1493,8 +1515,9 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     if ((flags & BOLT_FLAG_KERNEL_STAGED) && tn.staged == 0) tn.staged = 2;
     pl->tune = tn;
 
-    // Table sizing: (2 << load_shift - 1)x the expected groups (default 2x,
-    // load <= 0.5), grown on demand.
+    // Table sizing: the next power of two of (groups_hint << load_shift),
+    // load_shift 0..2 (autotuned; untuned 2), grown x8 when occupancy
+    // passes 3/4.
     uint64_t cap;
     if (cap_override) cap = cap_override;
     else if (d->groups_hint)
@@ -2426,7 +2449,7 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
     for (int block : {256, 512})
         for (int smem_shift : {0, 1, 8})
             for (int warp_agg : {0, 1})
-                for (int load_shift : {1, 2})
+                for (int load_shift : {0, 1, 2})
                     for (int smem_fill : {4, 6}) {
                         if (smem_shift == 8 && smem_fill != 4) continue;  // no shared tier: the fill is moot
                         cands.push_back({block, smem_shift, warp_agg, load_shift, smem_fill, 0, 0.0});
@@ -2434,7 +2457,7 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
     for (int staged : {1, 2, 4})
         for (int smem_shift : {0, 1})
             for (int warp_agg : {0, 1})
-                for (int load_shift : {1, 2}) cands.push_back({512, smem_shift, warp_agg, load_shift, 4, staged, 0.0});
+                for (int load_shift : {0, 1, 2}) cands.push_back({512, smem_shift, warp_agg, load_shift, 4, staged, 0.0});
     bolt_ctx::GbTune best{512, 1, 0, 2, 4, 0, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
@@ -2506,7 +2529,7 @@ extern "C" bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path) {
     while (std::fscanf(fp, "%llx %d %d %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift,
                        &t.smem_fill, &t.staged, &t.ms) == 8) {
         const bool valid = (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
-                           t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 1 &&
+                           t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 0 &&
                            t.load_shift <= 3 && t.smem_fill >= 1 && t.smem_fill <= 8 &&
                            (t.staged == 0 || t.staged == 1 || t.staged == 2 || t.staged == 4);
         if (valid) ctx->tune[(uint64_t)key] = t;
