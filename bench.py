@@ -88,6 +88,19 @@ def oracle_mod():
     return oracle
 
 
+def reduce_max(dist, v: float, device) -> float:
+    """Max of `v` over the ranks of the default process group (identity
+    without one). `device` holds the reduction tensor: the rank's GPU under
+    NCCL, the CPU under gloo."""
+    if not dist:
+        return v
+    import torch
+
+    t = torch.tensor([float(v)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peak_gbs():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -223,11 +236,7 @@ class Ctx:
             self.dist.barrier()
 
     def max_over_ranks(self, v: float) -> float:
-        if not self.dist:
-            return v
-        t = self.torch.tensor([v], device=self.dev)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(self.dist, v, self.dev)
 
     def check(self, what: str):
         st = self.lib.bolt_ctx_sync_status(self.eng._ctx, self.stream.cuda_stream)
