@@ -257,20 +257,23 @@ __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, in
     for (int j = 0; j < SORT_ITEMS; ++j) {
         const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
         const bool valid = e < n;
-        const uint32_t vm = __ballot_sync(0xffffffffu, valid);
-        rank[j] = 0;
-        if (valid) {
-            const uint32_t dg = (uint32_t)(key[j] >> shift) & 0xFFu;
-            const uint32_t peers = __match_any_sync(vm, dg);
-            const int leader = 31 - __clz(peers);
-            uint32_t b = 0;
-            if (lane == leader) {
-                b = warp_hist[w][dg];
-                warp_hist[w][dg] = b + __popc(peers);
-            }
-            b = __shfl_sync(vm, b, leader);
-            rank[j] = b + __popc(peers & lanemask_lt());
+        const uint32_t dg = valid ? (uint32_t)(key[j] >> shift) & 0xFFu : 0u;
+        // Lanes holding the same digit: one ballot per digit bit.
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int bit = 0; bit < 8; ++bit) {
+            const uint32_t on = (dg >> bit) & 1u;
+            const uint32_t bal = __ballot_sync(0xffffffffu, on);
+            peers &= on ? bal : ~bal;
         }
+        const int leader = valid ? 31 - __clz(peers) : (int)lane;
+        uint32_t b = 0;
+        if (valid && (int)lane == leader) {
+            b = warp_hist[w][dg];
+            warp_hist[w][dg] = b + __popc(peers);
+        }
+        b = __shfl_sync(0xffffffffu, b, leader);
+        rank[j] = valid ? b + __popc(peers & lanemask_lt()) : 0u;
         __syncwarp();
     }
     __syncthreads();
