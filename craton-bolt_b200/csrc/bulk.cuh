@@ -68,7 +68,7 @@ __device__ __forceinline__ uint64_t l2_evict_first_policy() {
 
 // Global -> shared bulk copy of `bytes` (a multiple of 16; both addresses
 // 16-byte aligned) that reports completion on `bar`. Into this CTA's own
-// shared memory only; no multicast.
+// shared memory only, from this GPU's own memory.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
                                           uint64_t policy) {
     asm volatile(

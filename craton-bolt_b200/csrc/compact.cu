@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
 
 }  // namespace
 
-bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& spec) {
+bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& spec, uint32_t flags) {
     CpArgs a{};
     a.sp = spec;
     // Stage the columns when a tile of them fits the budget and every input
@@ -262,12 +262,14 @@ bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& sp
         const uint64_t rows = spec.out_cap < spec.n ? spec.out_cap : spec.n;
         if (spec.col[c].out_valid) BOLT_CUDA(ctx, cudaMemsetAsync(spec.col[c].out_valid, 0, (rows + 7) / 8, s));
     }
+    kernel_mark_begin(ctx, flags, s);
     if (staged) {
         BOLT_CUDA(ctx, smem_optin(compact_kernel<true>, ctx));
         compact_kernel<true><<<(unsigned)ntiles, CP_BLOCK, stage_bytes, s>>>(a);
     } else {
         compact_kernel<false><<<(unsigned)ntiles, CP_BLOCK, 0, s>>>(a);
     }
+    kernel_mark_end(ctx, flags, s);
     ctx->last_launches++;
     BOLT_CUDA(ctx, cudaGetLastError());
     return BOLT_OK;
@@ -329,7 +331,7 @@ bolt_status compact_common(bolt_ctx* ctx, const bolt_col_view* cols, int32_t n_c
     ull* cnt = (ull*)arena_alloc(ctx, 256);
     if (!cnt) return fail(ctx, BOLT_ERR_CAPACITY, "compaction: scratch arena too small");
     sp.n_out_dev = cnt;
-    st = compact_enqueue(ctx, s, sp);
+    st = compact_enqueue(ctx, s, sp, flags);
     if (st != BOLT_OK) return st;
     st = call_end(ctx, flags, s);
     if (st != BOLT_OK) return st;

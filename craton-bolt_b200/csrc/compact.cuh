@@ -42,6 +42,7 @@ struct CompactSpec {
 };
 
 // Enqueues one fused predicate-evaluation + scan + scatter pass.
-bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& spec);
+// flags: BOLT_FLAG_PROFILE records the kernel's device time.
+bolt_status compact_enqueue(bolt_ctx* ctx, cudaStream_t s, const CompactSpec& spec, uint32_t flags = 0);
 
 }  // namespace bolt
