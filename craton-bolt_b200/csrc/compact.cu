@@ -198,33 +198,49 @@ __global__ void __launch_bounds__(CP_BLOCK) compact_kernel(const __grid_constant
     __syncthreads();
     if (STAGED) asm volatile("cp.async.wait_all;" ::: "memory");
     const ull tbase = s_base;
+    // Output row of each of this thread's kept rows (~0 when not kept or
+    // beyond the output capacity).
+    ull pos[CP_ITEMS];
 #pragma unroll
     for (int j = 0; j < CP_ITEMS; ++j) {
-        const uint64_t e = base + (uint64_t)j * CP_BLOCK + threadIdx.x;
         const uint32_t b = __ballot_sync(0xffffffffu, (keep >> j) & 1u);
-        if (!((keep >> j) & 1u)) continue;
-        const ull pos = tbase + cnt[j][w] + __popc(b & lanemask_lt());
-        if (pos >= sp.out_cap) continue;
-        const uint32_t slot = (uint32_t)j * CP_BLOCK + threadIdx.x;
-        for (int c = 0; c < sp.n_cols; ++c) {
-            const CompactCol& col = sp.col[c];
-            if (STAGED) {
-                const unsigned char* src = cp_stage + a.soff[c] + slot * (uint32_t)col.width;
-                switch (col.width) {
-                case 4: ((uint32_t*)col.out)[pos] = *reinterpret_cast<const uint32_t*>(src); break;
-                case 8: ((ull*)col.out)[pos] = *reinterpret_cast<const ull*>(src); break;
-                default: ((ulonglong2*)col.out)[pos] = *reinterpret_cast<const ulonglong2*>(src); break;
-                }
-            } else {
-                switch (col.width) {
-                case 4: ((uint32_t*)col.out)[pos] = __ldg((const uint32_t*)col.in + e); break;
-                case 8: ((ull*)col.out)[pos] = __ldg((const ull*)col.in + e); break;
-                default: ((ulonglong2*)col.out)[pos] = __ldg((const ulonglong2*)col.in + e); break;
-                }
-            }
-            if (col.out_valid && bit_valid(col.in_valid, e)) set_bit_atomic(col.out_valid, pos, true);
+        pos[j] = ~0ull;
+        if ((keep >> j) & 1u) {
+            const ull at = tbase + cnt[j][w] + __popc(b & lanemask_lt());
+            if (at < sp.out_cap) pos[j] = at;
         }
-        if (sp.row_ids) sp.row_ids[pos] = (sp.ids_in ? sp.ids_in[e] : (uint32_t)e) + sp.row_id_base;
+    }
+    // Column by column, so the width dispatch runs once per column.
+    for (int c = 0; c < sp.n_cols; ++c) {
+        const CompactCol& col = sp.col[c];
+        const int wd = col.width;
+#pragma unroll
+        for (int j = 0; j < CP_ITEMS; ++j) {
+            if (pos[j] == ~0ull) continue;
+            const uint64_t e = base + (uint64_t)j * CP_BLOCK + threadIdx.x;
+            const uint32_t slot = (uint32_t)j * CP_BLOCK + threadIdx.x;
+            const unsigned char* src = STAGED ? cp_stage + a.soff[c] + slot * (uint32_t)wd
+                                              : static_cast<const unsigned char*>(col.in) + e * (uint64_t)wd;
+            if (wd == 4) {
+                ((uint32_t*)col.out)[pos[j]] = STAGED ? *reinterpret_cast<const uint32_t*>(src)
+                                                      : __ldg(reinterpret_cast<const uint32_t*>(src));
+            } else if (wd == 8) {
+                ((ull*)col.out)[pos[j]] = STAGED ? *reinterpret_cast<const ull*>(src)
+                                                 : __ldg(reinterpret_cast<const ull*>(src));
+            } else {
+                ((ulonglong2*)col.out)[pos[j]] = STAGED ? *reinterpret_cast<const ulonglong2*>(src)
+                                                        : __ldg(reinterpret_cast<const ulonglong2*>(src));
+            }
+            if (col.out_valid && bit_valid(col.in_valid, e)) set_bit_atomic(col.out_valid, pos[j], true);
+        }
+    }
+    if (sp.row_ids) {
+#pragma unroll
+        for (int j = 0; j < CP_ITEMS; ++j) {
+            if (pos[j] == ~0ull) continue;
+            const uint64_t e = base + (uint64_t)j * CP_BLOCK + threadIdx.x;
+            sp.row_ids[pos[j]] = (sp.ids_in ? sp.ids_in[e] : (uint32_t)e) + sp.row_id_base;
+        }
     }
 }
 

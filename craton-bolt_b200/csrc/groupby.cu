@@ -1547,8 +1547,11 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         const uint64_t want = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * (d->groups_hint ? d->groups_hint : cap), 256));
         while (sl > 8 && (1ull << sl) > want) --sl;
         if (((size_t)1 << sl) * entry > budget) sl = 0;
+        // The tuned shrink (more CTAs per SM) applies when the expected
+        // groups outgrow the table anyway; a table that holds them all at
+        // the admission limit keeps its size.
         if (tn.smem_shift >= 8) sl = 0;
-        else if (sl) sl = std::max(sl - tn.smem_shift, 6);
+        else if (sl && (1ull << sl) < want) sl = std::max(sl - tn.smem_shift, 6);
     }
     p.smem_log2 = sl;
     p.smem_fill = sl ? (uint32_t)(((1ull << sl) * (uint64_t)tn.smem_fill) / 8) : 0;
