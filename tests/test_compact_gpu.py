@@ -12,7 +12,7 @@ from helpers import bitmap, unpack_bits
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [0, 1, 1000, 2048, 2049, 1_000_003])
+@pytest.mark.parametrize("n", [0, 1, 1000, 1023, 1024, 1025, 2048, 2049, 1_000_003])
 def test_compact_predicate(bolt, engine, oracle, n):
     rng = np.random.default_rng(n)
     f = rng.integers(0, 100, n).astype(np.int32)

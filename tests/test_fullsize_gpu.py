@@ -1,0 +1,125 @@
+"""GPU: every operator at the benchmark's full sizes, checked through
+properties that do not need the CPU oracle to run at that size (the oracle
+checks the same code paths bit-exactly at smaller sizes in the other files).
+
+* ORDER BY, 268,435,456 int64 keys: the output is a permutation, the keys
+  come out non-decreasing, equal keys keep their input order.
+* filtered two-key GROUP BY, 100M rows: group count = distinct filtered key
+  pairs, keys strictly ascending, COUNT total = filtered rows, per-group
+  AVG = SUM / COUNT, SUM total and global MIN / MAX against torch.
+* WHERE compaction, 100M rows x 5 columns: equal to torch's masked select.
+* join -> GROUP BY, 10M build x 200M probe: per-group COUNT and exact
+  Decimal128 SUM against an independent torch join (sorted build keys +
+  searchsorted).
+"""
+
+from __future__ import annotations
+
+import importlib
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def big_engine(bolt):
+    """An engine whose scratch arena holds the full-size sort buffers."""
+    eng = bolt.Engine(0, scratch_bytes=24 << 30)
+    yield eng
+    eng.close()
+
+
+def bench_mod():
+    if str(REPO) not in sys.path:
+        sys.path.insert(0, str(REPO))
+    return importlib.import_module("bench")
+
+
+def test_sort_i64_full_size_properties(bolt, big_engine):
+    dg = importlib.import_module("craton_bolt_b200.datagen")
+    n = 256 << 20
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    for s in range(0, n, 1 << 26):
+        m = min(1 << 26, n - s)
+        keys[s:s + m] = torch.from_numpy(dg.uniform_u64(4, 31, m, s).view(np.int64)).cuda()
+    perm = big_engine.sort_indices([bolt.Column(keys, "i64")], False, False).long()
+    assert perm.numel() == n
+    assert torch.equal(torch.sort(perm).values, torch.arange(n, device="cuda"))
+    sk = keys[perm]
+    assert bool((sk[1:] >= sk[:-1]).all())
+    ties = sk[1:] == sk[:-1]
+    assert bool((perm[1:][ties] > perm[:-1][ties]).all())
+
+
+def test_groupby_filtered_full_size_properties(bolt, big_engine):
+    b = bench_mod()
+    n = 100_000_000
+    data = b.gen_filtered(n, "cuda:0")
+    dev = {k: bolt.Column(torch.from_numpy(v).cuda(), b.FILTERED_DT[k]) for k, v in data.items()}
+    res = big_engine.execute_groupby(dev, ["a", "b"], b.FILTERED_AGGS, where=[("f", "<", 50)], groups_hint=4_000_000)
+    keep = dev["f"].data < 50
+    a = dev["a"].data[keep].long()
+    bb = dev["b"].data[keep].long()
+    packed = (a << 32) | (bb & 0xFFFFFFFF)
+    uniq = torch.unique(packed)
+    assert res.n_groups == uniq.numel()
+    ka = res.keys[0].data.long()
+    kb = res.keys[1].data.long()
+    kp = (ka << 32) | (kb & 0xFFFFFFFF)
+    assert bool((kp[1:] > kp[:-1]).all()) and torch.equal(kp, uniq)
+    s_vd, avg_vd, cnt, mn, mx = (c.data for c in res.aggs)
+    assert int(cnt.sum()) == int(keep.sum())
+    ok = cnt > 0
+    assert torch.allclose(avg_vd[ok], s_vd[ok] / cnt[ok].double(), rtol=1e-12, atol=0)
+    vd = dev["vd"].data[keep]
+    assert abs(float(s_vd.sum()) - float(vd.sum())) <= 1e-9 * float(vd.abs().sum())
+    vi = dev["vi"].data[keep]
+    assert int(mn.min()) == int(vi.min()) and int(mx.max()) == int(vi.max())
+
+
+def test_compact_full_size_equals_masked_select(bolt, big_engine):
+    b = bench_mod()
+    n = 100_000_000
+    data = b.gen_filtered(n, "cuda:0")
+    dev = {k: bolt.Column(torch.from_numpy(v).cuda(), b.FILTERED_DT[k]) for k, v in data.items()}
+    out, rows = big_engine.compact_columns(dev, where=[("f", "<", 50)])
+    keep = dev["f"].data < 50
+    assert torch.equal(rows.long(), torch.nonzero(keep).flatten())
+    for k, c in dev.items():
+        assert torch.equal(out[k].data, c.data[keep]), k
+
+
+def test_join_groupby_full_size_against_torch_join(bolt, big_engine):
+    dg = importlib.import_module("craton_bolt_b200.datagen")
+    nb, npr = 10_000_000, 200_000_000
+    bt = dg.join_build(nb, seed=3)
+    fk = torch.empty(npr, dtype=torch.int64, device="cuda")
+    amt = torch.empty((npr, 2), dtype=torch.int64, device="cuda")
+    for s in range(0, npr, 1 << 25):
+        ch = dg.join_probe(min(1 << 25, npr - s), nb, seed=3, start=s)
+        m = len(ch["fk"])
+        fk[s:s + m] = torch.from_numpy(ch["fk"]).cuda()
+        amt[s:s + m] = torch.from_numpy(ch["amount"]).cuda()
+    bk = torch.from_numpy(bt["k"]).cuda()
+    bg = torch.from_numpy(bt["g"]).cuda()
+    g, sums, counts = big_engine.join_groupby(bolt.Column(bk, "i64"), bolt.Column(bg, "i32"),
+                                              bolt.Column(fk, "i64"), bolt.Column(amt, "dec128", scale=2))
+    # Independent join: sorted build keys, searchsorted, exact int64 sums.
+    sk, order = torch.sort(bk)
+    pos = torch.searchsorted(sk, fk).clamp(max=nb - 1)
+    hit = sk[pos] == fk
+    grp = bg[order[pos[hit]]].long()
+    want_cnt = torch.bincount(grp, minlength=100)
+    want_sum = torch.zeros(100, dtype=torch.int64, device="cuda").scatter_add_(0, grp, amt[hit][:, 0])
+    present = torch.nonzero(want_cnt).flatten()
+    assert torch.equal(g.data.long(), present)
+    assert torch.equal(counts.data, want_cnt[present])
+    assert torch.equal(sums.data[:, 0], want_sum[present])
+    assert bool((sums.data[:, 1] == 0).all())

@@ -103,7 +103,7 @@ def test_sort_multi_key(bolt, engine, oracle):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("n", [0, 1, 2, 4095, 4096, 4097, 65537])
+@pytest.mark.parametrize("n", [0, 1, 2, 3071, 3072, 3073, 9217, 65537])
 def test_sort_edge_sizes(bolt, engine, oracle, n):
     v = np.random.default_rng(n).integers(-3, 3, n).astype(np.int64)
     check(bolt, engine, oracle, v, "i64")
