@@ -23,6 +23,7 @@ struct CompactPred {
     int32_t cmp;
     ll lit_i;
     double lit_f;
+    int32_t col_idx;  // index of the conjunct's column among the output columns
 };
 
 struct CompactSpec {

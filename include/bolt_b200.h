@@ -90,7 +90,8 @@ typedef struct bolt_ctx bolt_ctx;
 #define BOLT_FLAG_FORCE_GLOBAL 0x4u  /* GROUP BY: skip the shared-memory tier (testing) */
 #define BOLT_FLAG_FORCE_SHMEM  0x8u  /* GROUP BY: shared-memory tier only; spill -> BOLT_ERR_SPILL */
 #define BOLT_FLAG_NO_TUNE      0x10u /* GROUP BY: ignore the context's autotuned choices */
-#define BOLT_FLAG_KERNEL_REGS  0x20u /* GROUP BY: aggregate with the register-tile kernel (testing) */
+#define BOLT_FLAG_KERNEL_REGS  0x20u /* GROUP BY: aggregate with the register-tile kernel; compaction: per-element
+                                       copies instead of bulk-staged tiles (testing) */
 #define BOLT_FLAG_KERNEL_STAGED 0x40u /* GROUP BY: aggregate with the staged kernel where it applies (testing) */
 
 /* ------------------------------------------------------------------------ */
