@@ -101,3 +101,52 @@ def test_join_groupby_wide_decimal_and_overflow(bolt, engine, oracle):
         engine.join_groupby(bolt.col(bk[:2], "i64").to("cuda"), bolt.col(np.zeros(2, np.int32), "i32").to("cuda"),
                             bolt.col(np.array([0, 1], np.int64), "i64").to("cuda"),
                             bolt.col(np.stack([lo, hi], axis=1), "dec128").to("cuda"))
+
+
+def _join_groupby_vs_oracle(bolt, engine, oracle, bk, bg, pk, amt, kdt="i64", bvalid=None, pvalid=None):
+    bkc = bolt.col(bk, kdt, bitmap(bvalid) if bvalid is not None else None).to("cuda")
+    pkc = bolt.col(pk, kdt, bitmap(pvalid) if pvalid is not None else None).to("cuda")
+    g, s, c = engine.join_groupby(bkc, bolt.col(bg, "i32").to("cuda"), pkc, bolt.col(amt, "dec128").to("cuda"))
+    wg, wlo, whi, wc = oracle.join_groupby(
+        oracle.HostCol(bk, kdt, bitmap(bvalid) if bvalid is not None else None), bg,
+        oracle.HostCol(pk, kdt, bitmap(pvalid) if pvalid is not None else None), oracle.HostCol(amt, "dec128"))
+    assert np.array_equal(g.numpy(), wg)
+    sd = s.numpy()
+    assert np.array_equal(sd[:, 0], wlo) and np.array_equal(sd[:, 1], whi)
+    assert np.array_equal(c.numpy(), wc)
+
+
+@pytest.mark.parametrize("span", ["narrow_negative", "full_int32"])
+def test_join_groupby_payload_ranges(bolt, engine, oracle, span):
+    """Group payloads in a narrow negative range and over the whole int32
+    range (extremes included) equal the oracle."""
+    rng = np.random.default_rng(21)
+    nb, npr = 50_000, 400_000
+    bk = rng.permutation(np.arange(-nb, nb, 2, dtype=np.int64) * 7919)
+    if span == "narrow_negative":
+        bg = rng.integers(-60, 40, len(bk)).astype(np.int32)
+    else:
+        pool = np.array([-(2**31), 2**31 - 1, 0, -1, 123456789], np.int32)
+        bg = pool[rng.integers(0, len(pool), len(bk))]
+    pk = np.where(rng.random(npr) < 0.8, bk[rng.integers(0, len(bk), npr)], rng.integers(-(2**40), 2**40, npr))
+    amt = np.stack([rng.integers(0, 10**7, npr), np.zeros(npr, np.int64)], axis=1).astype(np.int64)
+    _join_groupby_vs_oracle(bolt, engine, oracle, bk, bg, pk, amt)
+
+
+@pytest.mark.parametrize("kdt", ["i32", "i64"])
+def test_join_groupby_extreme_keys_and_nulls(bolt, engine, oracle, kdt):
+    """Keys -1, 0 and the dtype's extremes, NULL build and probe keys."""
+    rng = np.random.default_rng(22)
+    info = np.iinfo(np.int32 if kdt == "i32" else np.int64)
+    special = np.array([-1, 0, info.min, info.max, 1, -2], dtype=np.int64)
+    rest = rng.choice(np.arange(10, 200_000, dtype=np.int64), 20_000, replace=False)
+    bk = np.concatenate([special, rest]).astype(np.int32 if kdt == "i32" else np.int64)
+    bg = rng.integers(0, 7, len(bk)).astype(np.int32)
+    npr = 150_000
+    pk = bk[rng.integers(0, len(bk), npr)].copy()
+    pk[::97] = -5  # absent
+    bvalid = rng.random(len(bk)) > 0.05
+    pvalid = rng.random(npr) > 0.05
+    amt = np.stack([rng.integers(-10**6, 10**6, npr), np.zeros(npr, np.int64)], axis=1).astype(np.int64)
+    amt[:, 1] = amt[:, 0] >> 63
+    _join_groupby_vs_oracle(bolt, engine, oracle, bk, bg, pk, amt, kdt, bvalid, pvalid)
