@@ -6,7 +6,8 @@
 //   * one histogram kernel reads the keys once and counts all digit
 //     positions of every segment (8-bit digits: 4 passes for 32-bit keys,
 //     8 for 64-bit);
-//   * one kernel per digit: tiles of 3072 keys are taken in arrival order
+//   * one kernel per digit: tiles of 3072 (64-bit) or 5120 (32-bit) keys are
+//     taken in arrival order
 //     from a flattened (segment, tile) list, ranked per warp with
 //     __match_any_sync (stable: element order within a warp's segment of the
 //     tile, warps in order), their digit counts chained across the segment's
@@ -27,8 +28,11 @@ namespace bolt {
 namespace {
 
 constexpr int SORT_BLOCK = 256;
-constexpr int SORT_ITEMS = 12;
-constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
+// Keys per thread in a pass: 32-bit keys leave registers and shared memory
+// for larger tiles (fewer tiles to chain, more independent loads per thread).
+constexpr int SORT_ITEMS_32 = 20;
+constexpr int SORT_ITEMS_64 = 12;
+constexpr int SORT_TILE_MIN = SORT_BLOCK * SORT_ITEMS_64;
 constexpr int HIST_CHUNK = 16384;
 constexpr uint32_t LB_AGG = 1u << 30;
 constexpr uint32_t LB_INC = 2u << 30;
@@ -37,8 +41,16 @@ constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
 constexpr int LB_WINDOW = 8;  // look-back words read per round trip
 
 template <typename K> struct KeyTraits;
-template <> struct KeyTraits<uint32_t> { static constexpr int NPASS = 4; };
-template <> struct KeyTraits<ull> { static constexpr int NPASS = 8; };
+template <> struct KeyTraits<uint32_t> {
+    static constexpr int NPASS = 4;
+    static constexpr int ITEMS = SORT_ITEMS_32;
+    static constexpr int TILE = SORT_BLOCK * ITEMS;
+};
+template <> struct KeyTraits<ull> {
+    static constexpr int NPASS = 8;
+    static constexpr int ITEMS = SORT_ITEMS_64;
+    static constexpr int TILE = SORT_BLOCK * ITEMS;
+};
 
 struct SegDesc {
     const void* keys;
@@ -195,6 +207,8 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(SortArgs a) {
 template <typename K>
 __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, int p) {
     constexpr int NW = SORT_BLOCK / 32;
+    constexpr int SORT_ITEMS = KeyTraits<K>::ITEMS;
+    constexpr int SORT_TILE = KeyTraits<K>::TILE;
     __shared__ uint32_t s_item;
     __shared__ uint32_t warp_hist[NW][256];
     __shared__ uint32_t tile_off[256];
@@ -382,6 +396,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, in
 template <typename K>
 bolt_status run_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
     constexpr int NP = KeyTraits<K>::NPASS;
+    constexpr int SORT_TILE = KeyTraits<K>::TILE;
     const int nseg = (int)sp.segs.size();
     if (nseg == 0) return BOLT_OK;
     std::vector<SegDesc> segs(nseg);
@@ -454,7 +469,7 @@ bolt_status run_sort(bolt_ctx* ctx, cudaStream_t s, const SortSpec& sp) {
 
 uint64_t radix_sort_scratch(uint64_t total_n, uint64_t nseg, int32_t src) {
     const uint64_t ksz = (src == SRC_I32 || src == SRC_F32 || src == SRC_U32) ? 4 : 8;
-    const uint64_t items = total_n / SORT_TILE + nseg + 1;
+    const uint64_t items = total_n / SORT_TILE_MIN + nseg + 1;
     return 2 * total_n * (ksz + 4) + 2 * items * 256 * 4 + nseg * (2 * 8 * 256 * 4 + 96) + 64 * 1024;
 }
 

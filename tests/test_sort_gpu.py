@@ -105,8 +105,17 @@ def test_sort_multi_key(bolt, engine, oracle):
 
 @pytest.mark.parametrize("n", [0, 1, 2, 3071, 3072, 3073, 9217, 65537])
 def test_sort_edge_sizes(bolt, engine, oracle, n):
+    """Tile boundaries of 64-bit keys (3,072 keys per tile)."""
     v = np.random.default_rng(n).integers(-3, 3, n).astype(np.int64)
     check(bolt, engine, oracle, v, "i64")
+
+
+@pytest.mark.parametrize("dt", ["i32", "f32"])
+@pytest.mark.parametrize("n", [5119, 5120, 5121, 15361, 65537])
+def test_sort_edge_sizes_32bit(bolt, engine, oracle, n, dt):
+    """Tile boundaries of 32-bit keys (5,120 keys per tile)."""
+    v = np.random.default_rng(n).integers(-3, 3, n)
+    check(bolt, engine, oracle, v.astype(np.int32 if dt == "i32" else np.float32), dt)
 
 
 def test_sort_constant_keys_is_identity(bolt, engine, oracle):
