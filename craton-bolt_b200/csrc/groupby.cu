@@ -210,21 +210,72 @@ __device__ __forceinline__ void merge_words(ull* w, int kind, ull c0, ull c1) {
     }
 }
 
-// Row-path merge into the shared-memory tier. Shared 64-bit atomic add and
-// max are compare-and-swap loops that serialise when lanes of a warp (or
-// several warps) hit one hot group, while 32-bit reductions are native and
-// combine same-address lanes. So COUNT accumulates in the low 32 bits of its
-// word (exact while a CTA's table sees fewer than 2^32 rows: cnt32), and
-// MIN / MAX read the word first and only CAS when the row would win, which
-// for a hot group is rarely after its first few rows.
+// Exact 64-bit add into a shared-memory word through native 32-bit atomics.
+// A 64-bit shared atomic add is a compare-and-swap loop: about 6x the cost
+// of a 32-bit add when uncontended and thousands of cycles when a warp or
+// several warps hit one hot group. Here the low half takes the value's low
+// 32 bits and its returned old value says whether it wrapped; the high half
+// takes the high 32 bits plus that carry. The adds are linearisable, so the
+// carries sum to exactly the wraps of the low half and the word ends equal
+// to the 64-bit sum (it is only read after the CTA's final barrier).
+__device__ __forceinline__ void smem_add64(ull* w, ull v) {
+    uint32_t* h = reinterpret_cast<uint32_t*>(w);
+    const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+    uint32_t c = 0;
+    if (lo) {
+        const uint32_t o = atomicAdd(h, lo);
+        c = (o + lo < o) ? 1u : 0u;
+    }
+    if (hi + c) atomicAdd(h + 1, hi + c);
+}
+
+// The same, returning the carry out of bit 63 (the high half's add then
+// returns its old value), for the low word of a 128-bit sum.
+__device__ __forceinline__ uint32_t smem_add64_carry(ull* w, ull v) {
+    uint32_t* h = reinterpret_cast<uint32_t*>(w);
+    const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+    uint32_t c = 0;
+    if (lo) {
+        const uint32_t o = atomicAdd(h, lo);
+        c = (o + lo < o) ? 1u : 0u;
+    }
+    const uint32_t up = hi + c;
+    uint32_t out = (up < hi) ? 1u : 0u;  // hi + c wrapped to 0: carry out, nothing to add
+    if (up) {
+        const uint32_t o = atomicAdd(h + 1, up);
+        out += (o + up < o) ? 1u : 0u;
+    }
+    return out;
+}
+
+// Row-path merge into the shared-memory tier. Sums go through 32-bit
+// atomics (smem_add64); COUNT accumulates in the low 32 bits of its word
+// (exact while a CTA's table sees fewer than 2^32 rows: cnt32), and MIN /
+// MAX read the word first and only use the (native) 64-bit atomic max when
+// the row would win, which for a hot group is rarely after its first rows.
 __device__ __forceinline__ void merge_words_smem(ull* w, int kind, ull c0, ull c1, bool cnt32) {
     if ((c0 | c1) == 0) return;
-    if (kind == K_COUNT && cnt32) {
-        atomicAdd(reinterpret_cast<uint32_t*>(w), (uint32_t)c0);
-    } else if (kind == K_MAX_ORD || kind == K_MIN_ORD) {
+    switch (kind) {
+    case K_COUNT:
+        if (cnt32) atomicAdd(reinterpret_cast<uint32_t*>(w), (uint32_t)c0);
+        else smem_add64(w, c0);
+        break;
+    case K_SUM_I32: smem_add64(w, c0); break;
+    case K_SUM_I64:
+    case K_SUM_D64:
+        if (c0) smem_add64(w, c0);
+        if (c1) smem_add64(w + 1, c1);
+        break;
+    case K_SUM_FX: {
+        const uint32_t carry = c0 ? smem_add64_carry(w, c0) : 0u;
+        if (c1 + carry) smem_add64(w + 1, c1 + carry);
+        break;
+    }
+    case K_MAX_ORD:
+    case K_MIN_ORD:
         if (c0 > *reinterpret_cast<volatile ull*>(w)) atomicMax(w, c0);
-    } else {
-        merge_words(w, kind, c0, c1);
+        break;
+    default: merge_words(w, kind, c0, c1); break;  // D128, f64 atomics: rare modes
     }
 }
 
