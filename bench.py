@@ -350,6 +350,21 @@ class PreparedCall:
         return int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
 
 
+def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
+    """Which aggregation kernel the timed GROUP BY runs: the staged kernel
+    when the tuning cache (or, untuned, the library's default for inputs
+    of 4M rows and more) chooses it, else the register-tile kernel."""
+    staged = rows >= (1 << 22)
+    if tuned:
+        import tempfile
+        with tempfile.NamedTemporaryFile("r", suffix=".txt") as f:
+            c.eng.save_tuning(f.name)
+            lines = [ln.split() for ln in open(f.name) if ln.strip() and not ln.startswith("#")]
+        if len(lines) == 1 and len(lines[0]) >= 8:
+            staged = int(lines[0][6]) > 0
+    return "gb_staged_kernel" if staged else "gb_agg_kernel"
+
+
 def cpu_rows_per_s_groupby(table_np: dict, dts: dict, group_by, aggs, where, n_sample: int):
     orc = oracle_mod()
     host = {k: orc.HostCol(np.ascontiguousarray(v[:n_sample]), dts[k]) for k, v in table_np.items()}
@@ -381,12 +396,13 @@ def w_groupby_filtered(c: Ctx):
         progress(f"autotuned: {best:.3f} ms")
     if a.save_tuning:
         c.eng.save_tuning(a.save_tuning)
+    kernel = agg_kernel_name(c, a.rows, tuned is not None)
     call = PreparedCall(c, pq)
     ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
     n_groups = int(call.ng.item())
     progress(f"timed: {ms / a.steps:.3f} ms/step, {n_groups} groups")
     alg = a.rows * FILTERED_BYTES
-    line = base_line(c, ms, a.rows, alg, kms, "gb_agg_kernel", "groupby_filtered",
+    line = base_line(c, ms, a.rows, alg, kms, kernel, "groupby_filtered",
                      {"workload": "filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) ranks, "
                                   "WHERE f < 50, SUM/AVG(vd f64), COUNT(*), MIN/MAX(vi i64)",
                       "rows": a.rows, "groups": n_groups, "groups_hint": a.groups_hint,

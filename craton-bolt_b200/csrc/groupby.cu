@@ -2511,7 +2511,8 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
     for (int staged : {1, 2, 4})
         for (int smem_shift : {0, 1})
             for (int warp_agg : {0, 1})
-                for (int load_shift : {0, 1, 2}) cands.push_back({512, smem_shift, warp_agg, load_shift, 4, staged, 0.0});
+                for (int load_shift : {0, 1, 2})
+                    for (int smem_fill : {4, 6}) cands.push_back({512, smem_shift, warp_agg, load_shift, smem_fill, staged, 0.0});
     bolt_ctx::GbTune best{512, 1, 0, 2, 4, 0, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
