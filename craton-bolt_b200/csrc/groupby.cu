@@ -1551,8 +1551,13 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     for (int a = 0; a < d->n_aggs; ++a) out_cap = std::min<uint64_t>(out_cap, out->aggs[a].cap);
     f.out_cap = out_cap;
 
+    // A query has at most as many groups as rows (plus the NULL group), so a
+    // hint above the row count sizes nothing larger than the rows need: a
+    // 10K-row query hinted at 1M groups would otherwise clear and scan an
+    // 8M-slot table.
+    const uint64_t hint = d->groups_hint ? std::min<uint64_t>(d->groups_hint, n + 2) : 0;
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
-    pl->shape = gb_shape_key(p, n, d->groups_hint);
+    pl->shape = gb_shape_key(p, n, hint);
     // Untuned default: the register kernel for small inputs, the staged
     // kernel (2 chunks per consumer warp) from 4M rows, where its pipeline
     // fills.
@@ -1571,8 +1576,8 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     // passes 3/4.
     uint64_t cap;
     if (cap_override) cap = cap_override;
-    else if (d->groups_hint)
-        cap = 1ull << ceil_log2_u64(std::max<uint64_t>((d->groups_hint << tn.load_shift) + 16, 64));
+    else if (hint)
+        cap = 1ull << ceil_log2_u64(std::max<uint64_t>((hint << tn.load_shift) + 16, 64));
     else cap = 1ull << ceil_log2_u64(std::max<uint64_t>(std::min<uint64_t>(2 * n + 16, 1ull << 16), 64));
     pl->cap = cap;
     p.log2cap = f.log2cap = ceil_log2_u64(cap);
@@ -1595,7 +1600,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     int sl = 0;
     if (!(flags & BOLT_FLAG_FORCE_GLOBAL)) {
         while (((size_t)2 << sl) * entry <= budget && sl < 16) ++sl;
-        const uint64_t want = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * (d->groups_hint ? d->groups_hint : cap), 256));
+        const uint64_t want = 1ull << ceil_log2_u64(std::max<uint64_t>(2 * (hint ? hint : cap), 256));
         while (sl > 8 && (1ull << sl) > want) --sl;
         if (((size_t)1 << sl) * entry > budget) sl = 0;
         // The tuned shrink (more CTAs per SM) applies when the expected
@@ -1920,8 +1925,8 @@ extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64
     // two-word sum and a count); slots as the planner sizes them untuned
     // (4x the expected groups, or 2x the rows up to 64K without a hint).
     const uint64_t words = 1 + 3ull * (uint64_t)(desc->n_aggs > 0 ? desc->n_aggs : 1);
-    const uint64_t want = desc->groups_hint ? (desc->groups_hint << 2) + 16
-                                            : std::min<uint64_t>(2 * n_rows + 16, 1ull << 16);
+    const uint64_t hint = desc->groups_hint ? std::min<uint64_t>(desc->groups_hint, n_rows + 2) : 0;
+    const uint64_t want = hint ? (hint << 2) + 16 : std::min<uint64_t>(2 * n_rows + 16, 1ull << 16);
     const uint64_t cap = 1ull << ceil_log2_u64(std::max<uint64_t>(want, 64));
     uint64_t bytes = (cap + 2) * words * 8 + 4096;
     if (cap > 8192) bytes += (cap + 1) * 16 + radix_sort_scratch(cap + 1, 1, SRC_U64_KEYS);
