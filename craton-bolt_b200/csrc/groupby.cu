@@ -1561,7 +1561,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     // Untuned default: the register kernel for small inputs, the staged
     // kernel (2 chunks per consumer warp) from 4M rows, where its pipeline
     // fills.
-    bolt_ctx::GbTune tn{512, 1, 0, 2, 4, n >= (1ull << 22) ? 2 : 0, 0.0};
+    bolt_ctx::GbTune tn{512, 1, 0, 1, 4, n >= (1ull << 22) ? 2 : 0, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
@@ -1572,7 +1572,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     pl->tune = tn;
 
     // Table sizing: the next power of two of (groups_hint << load_shift),
-    // load_shift 0..2 (autotuned; untuned 2), grown x8 when occupancy
+    // load_shift 0..2 (autotuned; untuned 1), grown x8 when occupancy
     // passes 3/4.
     uint64_t cap;
     if (cap_override) cap = cap_override;
@@ -1923,10 +1923,10 @@ extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64
     if (!desc) return 0;
     // Table words per slot: key + at most three words per aggregate (AVG: a
     // two-word sum and a count); slots as the planner sizes them untuned
-    // (4x the expected groups, or 2x the rows up to 64K without a hint).
+    // (2x the expected groups, or 2x the rows up to 64K without a hint).
     const uint64_t words = 1 + 3ull * (uint64_t)(desc->n_aggs > 0 ? desc->n_aggs : 1);
     const uint64_t hint = desc->groups_hint ? std::min<uint64_t>(desc->groups_hint, n_rows + 2) : 0;
-    const uint64_t want = hint ? (hint << 2) + 16 : std::min<uint64_t>(2 * n_rows + 16, 1ull << 16);
+    const uint64_t want = hint ? (hint << 1) + 16 : std::min<uint64_t>(2 * n_rows + 16, 1ull << 16);
     const uint64_t cap = 1ull << ceil_log2_u64(std::max<uint64_t>(want, 64));
     uint64_t bytes = (cap + 2) * words * 8 + 4096;
     if (cap > 8192) bytes += (cap + 1) * 16 + radix_sort_scratch(cap + 1, 1, SRC_U64_KEYS);
@@ -2518,7 +2518,7 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             for (int warp_agg : {0, 1})
                 for (int load_shift : {0, 1, 2})
                     for (int smem_fill : {4, 6}) cands.push_back({512, smem_shift, warp_agg, load_shift, smem_fill, staged, 0.0});
-    bolt_ctx::GbTune best{512, 1, 0, 2, 4, 0, 1e30};
+    bolt_ctx::GbTune best{512, 1, 0, 1, 4, 0, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
     for (auto& c : cands) {

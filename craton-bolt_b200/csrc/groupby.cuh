@@ -149,7 +149,7 @@ struct GbPlan {
     uint32_t flags = 0;
     ull* words = nullptr;  // device: [0] occupancy, [1] non-NULL groups, [2] groups, [3] status
     uint64_t shape = 0;    // autotuning key of the query shape
-    bolt_ctx::GbTune tune{512, 1, 0, 2, 4, 0, 0.0};
+    bolt_ctx::GbTune tune{512, 1, 0, 1, 4, 0, 0.0};
 };
 
 // Key of a query shape for the autotuning cache: key / predicate / state
