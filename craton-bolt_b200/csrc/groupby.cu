@@ -190,12 +190,18 @@ __device__ __forceinline__ void merge_words(ull* w, int kind, ull c0, ull c1) {
         if (c0) atomicAdd(w, c0);
         if (c1) atomicAdd(w + 1, c1);
         break;
-    case K_SUM_FX: {
-        ull old = c0 ? atomicAdd(w, c0) : 0ull;
-        ull carry = (c0 && old + c0 < old) ? 1ull : 0ull;
-        if (c1 + carry) atomicAdd(w + 1, c1 + carry);
+    case K_SUM_FX:
+        // Global layout: bits 0-31 and 32-63 of the low word and the signed
+        // high word accumulate in separate words, so no add waits for a
+        // result (a 128-bit add would need the low word's old value for its
+        // carry, one more round trip for every row that misses the shared
+        // tier). The sums stay exact: the first two are below n * 2^32, the
+        // third below 2^62 in magnitude (the fixed-point window shrinks as
+        // the row count grows, see f64_to_fixed's scale).
+        if (c0 & 0xFFFFFFFFull) atomicAdd(w, c0 & 0xFFFFFFFFull);
+        if (c0 >> 32) atomicAdd(w + 1, c0 >> 32);
+        if (c1) atomicAdd(w + 2, c1);
         break;
-    }
     case K_SUM_D128: {
         ull old = c0 ? atomicAdd(w, c0) : 0ull;
         ull carry = (c0 && old + c0 < old) ? 1ull : 0ull;
@@ -279,7 +285,9 @@ __device__ __forceinline__ void merge_words_smem(ull* w, int kind, ull c0, ull c
     }
 }
 
-// Folds a partial state (all of its words) into state words w.
+// Folds a shared-table state (its words at src) into global-table state
+// words w. A shared K_SUM_FX state is the 128-bit sum (lo, hi), which
+// merge_words splits into the global layout.
 __device__ __forceinline__ void merge_partial(ull* w, int kind, const ull* src) {
     if (kind == K_SUM_D128) {
         const ull s0 = src[0];
@@ -394,7 +402,7 @@ template <int MAXS, class SP>
 __device__ __forceinline__ void row_fold(const GbParams& p, ull* sk, ull* sw, int C, uint32_t* fill, bool row_in,
                                          bool knull, ull stored, const ull (&raw)[MAXS], uint32_t vbits,
                                          uint32_t dfit, uint64_t r, uint32_t& inserts, uint32_t& absbits) {
-    const int SW = p.slot_words - 1;
+    const int SW = p.sslot_words - 1;
     const uint32_t lane = lane_id();
     const int NS = snum<SP>(p);
     bool row = row_in;
@@ -464,7 +472,7 @@ __device__ __forceinline__ void row_fold(const GbParams& p, ull* sk, ull* sw, in
         ull* w = sw + (ull)sl * SW - 1;  // state word offsets count the key word
 #pragma unroll
         for (int s = 0; s < MAXS; ++s)
-            if (s < NS) merge_words_smem(w + p.st[s].word, skind<SP>(p, s), c0[s], c1[s], p.cnt32);
+            if (s < NS) merge_words_smem(w + p.st[s].sword, skind<SP>(p, s), c0[s], c1[s], p.cnt32);
     } else {
         const int64_t g = g_find_insert(p, stored, inserts);
         if (g >= 0) {
@@ -600,7 +608,7 @@ __device__ __forceinline__ void gb_flush_absbits(const GbParams& p, uint32_t& ab
 // Merges a CTA's shared table into the query's global table (whole CTA,
 // after a __syncthreads()).
 __device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk, const ull* sw, int C) {
-    const int SW = p.slot_words - 1;
+    const int SW = p.sslot_words - 1;
     uint32_t inserts = 0;
     for (int i = threadIdx.x; i < C; i += blockDim.x) {
         const ull key = sk[i];
@@ -611,7 +619,7 @@ __device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk
         const ull* src = sw + (ull)i * SW - 1;
         for (int s = 0; s < p.n_st; ++s) {
             const StateDesc& d = p.st[s];
-            merge_partial(w + d.word, d.kind, src + d.word);
+            merge_partial(w + d.word, d.kind, src + d.sword);
         }
     }
     if (inserts) {
@@ -624,7 +632,7 @@ template <int U, int MAXS, class SP>
 __global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_agg_kernel(const __grid_constant__ GbParams p) {
     extern __shared__ __align__(16) ull smem[];
     __shared__ uint32_t s_fill;
-    const int SW = p.slot_words - 1;
+    const int SW = p.sslot_words - 1;
     const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
     ull* sk = smem;
     ull* sw = smem + C;
@@ -776,7 +784,7 @@ __global__ void __launch_bounds__(1024, 1) gb_staged_kernel(const __grid_constan
     const int NW = (int)(blockDim.x >> 5) - 1;  // consumer warps
     const int warp = (int)(threadIdx.x >> 5);
     const uint32_t lane = lane_id();
-    const int SW = p.slot_words - 1;
+    const int SW = p.sslot_words - 1;
     const int C = p.smem_log2 ? (1 << p.smem_log2) : 0;
     unsigned char* stages = dsm;
     ull* sk = reinterpret_cast<ull*>(dsm + (size_t)S * p.stage_bytes);
@@ -882,7 +890,11 @@ __device__ __forceinline__ double sum_as_double(const GbFinal& f, const StateDes
         __int128 v = ((__int128)(ll)w[1] << 32) + (__int128)w[0];
         return i128_to_double_scaled((ull)v, (ll)(v >> 64), 0);
     }
-    case K_SUM_FX: return i128_to_double_scaled(w[0], (ll)w[1], f.fx_e);
+    case K_SUM_FX: {  // global layout: w0 + w1 * 2^32 + w2 * 2^64, mod 2^128
+        const unsigned __int128 v =
+            (unsigned __int128)w[0] + ((unsigned __int128)w[1] << 32) + ((unsigned __int128)w[2] << 64);
+        return i128_to_double_scaled((ull)v, (ll)(ull)(v >> 64), f.fx_e);
+    }
     default: return __longlong_as_double((ll)w[0]);
     }
 }
@@ -1246,7 +1258,7 @@ __global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_batch_agg_kernel(
             for (int i = threadIdx.x; i < (int)(sizeof(GbParams) / 16); i += blockDim.x) dst[i] = src[i];
             __syncthreads();
             C = p.smem_log2 ? (1 << p.smem_log2) : 0;
-            for (int i = threadIdx.x; i < C * p.slot_words; i += blockDim.x) smem[i] = 0;
+            for (int i = threadIdx.x; i < C * p.sslot_words; i += blockDim.x) smem[i] = 0;
             if (threadIdx.x == 0) s_fill = 0;
             __syncthreads();
             cur = q;
@@ -1429,7 +1441,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         sd.kind = kind;
         sd.dtype = c ? c->dtype : BOLT_I64;
         sd.word = word;
-        sd.nwords = (kind == K_SUM_I64 || kind == K_SUM_FX || kind == K_SUM_D64) ? 2 : (kind == K_SUM_D128 ? 3 : 1);
+        sd.nwords = (kind == K_SUM_I64 || kind == K_SUM_D64) ? 2 : (kind == K_SUM_D128 || kind == K_SUM_FX ? 3 : 1);
         word += sd.nwords;
         return n_st++;
     };
@@ -1510,12 +1522,16 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
         std::stable_sort(order, order + n_st, [&](int a, int b) { return rank(p.st[a].kind) < rank(p.st[b].kind); });
         StateDesc sorted[GB_MAX_STATES];
         word = 1;
+        int sword = 1;
         for (int i = 0; i < n_st; ++i) {
             sorted[i] = p.st[order[i]];
             sorted[i].word = word;
+            sorted[i].sword = sword;
             word += sorted[i].nwords;
+            sword += sorted[i].nwords - (sorted[i].kind == K_SUM_FX ? 1 : 0);
             where[order[i]] = i;
         }
+        p.sslot_words = sword;
         for (int i = 0; i < n_st; ++i) p.st[i] = sorted[i];
         for (int a = 0; a < d->n_aggs; ++a) {
             AggOut& g = f.agg[a];
@@ -1595,7 +1611,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
 
     // Shared-memory tier: the largest power of two of slots that fits the
     // opt-in limit, no larger than 2x the expected groups.
-    const size_t entry = 8ull * (size_t)word;
+    const size_t entry = 8ull * (size_t)p.sslot_words;
     const size_t budget = (size_t)std::max(ctx->max_smem_optin - 2048, 0);
     int sl = 0;
     if (!(flags & BOLT_FLAG_FORCE_GLOBAL)) {
@@ -1671,7 +1687,7 @@ bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& pl, GbStagedLaunch* out
     const size_t budget = (size_t)std::max(ctx->max_smem_optin - 1024, 0);
     int sl = p.smem_log2;
     for (;;) {
-        const size_t table = sl ? ((size_t)1 << sl) * 8 * (size_t)p.slot_words : 0;
+        const size_t table = sl ? ((size_t)1 << sl) * 8 * (size_t)p.sslot_words : 0;
         if (table + lists + 2 * stage <= budget) {
             const int S = (int)std::min<size_t>(4, (budget - table - lists) / stage);
             if (out) *out = GbStagedLaunch{block, T, S, (uint32_t)stage, sl, (size_t)S * stage + table + lists};
@@ -1724,7 +1740,7 @@ static bolt_status gb_run_tables(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream
 // Launches the aggregation of one query (the single-query kernels).
 static bolt_status gb_agg_one(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags) {
     GbParams& p = pl->prm;
-    size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.slot_words;
+    size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.sslot_words;
     const uint64_t tile = (uint64_t)pl->block * pl->u;
     GbStagedLaunch stg;
     const bool staged = gb_staged_layout(ctx, *pl, &stg);
@@ -1777,7 +1793,7 @@ static bolt_status gb_agg_batch(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream_
     for (int q = 0; q < nq; ++q) {
         max_st = std::max(max_st, (int)pls[q]->prm.n_st);
         if (pls[q]->prm.spec != spec) spec = 0;
-        smem = std::max<size_t>(smem, (size_t)pls[q]->smem_entries * 8 * (size_t)pls[q]->prm.slot_words);
+        smem = std::max<size_t>(smem, (size_t)pls[q]->smem_entries * 8 * (size_t)pls[q]->prm.sslot_words);
     }
     if (spec == 0 && max_st > 4) u = 2;
     const BatchKernel kfn = batch_kernel_for(spec, max_st);
@@ -1921,10 +1937,10 @@ using namespace bolt;
 
 extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64_t n_rows) {
     if (!desc) return 0;
-    // Table words per slot: key + at most three words per aggregate (AVG: a
-    // two-word sum and a count); slots as the planner sizes them untuned
+    // Table words per slot: key + at most four words per aggregate (AVG: a
+    // three-word sum and a count); slots as the planner sizes them untuned
     // (2x the expected groups, or 2x the rows up to 64K without a hint).
-    const uint64_t words = 1 + 3ull * (uint64_t)(desc->n_aggs > 0 ? desc->n_aggs : 1);
+    const uint64_t words = 1 + 4ull * (uint64_t)(desc->n_aggs > 0 ? desc->n_aggs : 1);
     const uint64_t hint = desc->groups_hint ? std::min<uint64_t>(desc->groups_hint, n_rows + 2) : 0;
     const uint64_t want = hint ? (hint << 1) + 16 : std::min<uint64_t>(2 * n_rows + 16, 1ull << 16);
     const uint64_t cap = 1ull << ceil_log2_u64(std::max<uint64_t>(want, 64));
@@ -2326,7 +2342,7 @@ extern "C" bolt_status bolt_groupby_noalloc(const bolt_groupby_desc* desc, bolt_
             return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: clearing the static scratch failed");
         if (cudaMemcpyAsync(d_final, &f, sizeof(GbFinal), cudaMemcpyHostToDevice, s) != cudaSuccess)
             return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: descriptor upload failed");
-        const size_t smem = (size_t)pl.smem_entries * 8ull * (size_t)p.slot_words;
+        const size_t smem = (size_t)pl.smem_entries * 8ull * (size_t)p.sslot_words;
         const uint64_t tile = (uint64_t)pl.block * pl.u;
         const uint64_t tiles = (p.n_rows + tile - 1) / tile;
         const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)c.num_sms, std::max<uint64_t>(tiles, 1));

@@ -12,7 +12,9 @@ enum StKind : int32_t {
     K_COUNT = 0,      // 1 word: count of valid inputs (or rows)
     K_SUM_I32 = 1,    // 1 word: i64 sum of i32 inputs
     K_SUM_I64 = 2,    // 2 words: sum of low 32 bits (u64), sum of high 32 bits (i64)
-    K_SUM_FX = 3,     // 2 words: i128 fixed-point sum (lo with carry, hi)
+    K_SUM_FX = 3,     // i128 fixed-point sum. Global table, 3 words updated without returning
+                      // adds: sums of bits 0-31, of bits 32-63 and of the signed high word
+                      // of the contributions. Shared table, 2 words: lo with carry, hi.
     K_SUM_FATOM = 4,  // 1 word: f64 atomicAdd (fallback for non-finite / huge values)
     K_MAX_ORD = 5,    // 1 word: max of an order-preserving u64 image
     K_MIN_ORD = 6,    // 1 word: max of the bitwise NOT of that image
@@ -31,8 +33,10 @@ struct StateDesc {
     const uint8_t* valid;
     int32_t kind;
     int32_t dtype;
-    int32_t word;    // offset of the state's first word inside the slot (key is word 0)
+    int32_t word;    // offset of the state's first word inside a global-table slot (key is word 0)
     int32_t nwords;
+    int32_t sword;   // the same inside a shared-table slot (K_SUM_FX is one word shorter there)
+    int32_t pad;
 };
 
 struct PredDesc {
@@ -68,7 +72,9 @@ struct alignas(16) GbParams {
     PredDesc pred[GB_MAX_PREDS];
     StateDesc st[GB_MAX_STATES];
     int32_t n_st;
-    int32_t slot_words;
+    int32_t slot_words;  // words per global-table slot
+    int32_t sslot_words; // words per shared-table slot
+    int32_t pad_s;
     uint64_t row_begin;
     uint64_t n_rows;
     ull* gtab;           // (cap + 2) * slot_words words; slot cap = key -1, cap + 1 = NULL key
