@@ -89,3 +89,19 @@ def test_no_gpu_gives_typed_error(lib):
 def test_null_context_is_rejected(lib):
     assert lib.bolt_groupby(None, None, None, 0, None) == 7
     assert lib.bolt_radix_sort_perm(None, None, 0, 0, None, 0, None) == 7
+
+
+def test_footprint_tracks_rows_not_only_the_hint(lib):
+    """The admission footprint (host arithmetic, no GPU) sizes the table from
+    min(groups hint, rows): a small query hinted at many groups stays small,
+    and the footprint never shrinks as rows grow."""
+    from importlib import import_module
+    load_bolt()
+    abi = import_module("craton_bolt_b200._abi")
+    aggs = (abi.AggSpec * 2)(abi.AggSpec(0, 1), abi.AggSpec(1, -1))
+    d = abi.GroupbyDesc(None, 2, None, 1, None, 0, aggs, 2, 1_000_000)
+    small = lib.bolt_groupby_footprint(C.byref(d), 10_000)
+    big = lib.bolt_groupby_footprint(C.byref(d), 50_000_000)
+    assert small < big / 50
+    sizes = [lib.bolt_groupby_footprint(C.byref(d), n) for n in (1, 100, 10_000, 1_000_000, 10_000_000)]
+    assert sizes == sorted(sizes)
