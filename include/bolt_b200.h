@@ -302,7 +302,9 @@ bolt_status bolt_radix_sort_perm_multi(bolt_ctx* ctx, const bolt_col_view* keys,
 /* conjunction, input order preserved.                                        */
 /* Replaces gpu_compact::compact_columns_on_gpu (src/exec/gpu_compact.rs:1005)*/
 /* with prefix_scan_mask (gpu_compact.rs:415) and the predicate kernel        */
-/* (scan_kernel.rs:265) fused into one decoupled look-back pass.              */
+/* (scan_kernel.rs:265) fused: one decoupled look-back pass, or for inputs of */
+/* 4M rows and more a count pass over the WHERE columns, a scan of the tile  */
+/* counts and a scatter pass that stages whole tiles with bulk copies.        */
 /* `out[c]` receives column c (validity carried); `row_ids` (nullable, U32)   */
 /* receives the selected row indices.                                          */
 /* ------------------------------------------------------------------------ */
