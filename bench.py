@@ -688,7 +688,7 @@ def w_batch(c: Ctx):
             prepared2 = [prep(q) for q in qs]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            tickets = [srv.submit(pq) for pq in prepared2]
+            tickets = srv.submit_many(prepared2)  # the whole burst in one call
             for t in tickets:
                 srv.wait(t)
             batch_s = time.perf_counter() - t0

@@ -598,10 +598,27 @@ class Server:
         self._pending[int(t.value)] = (pq, q)
         return int(t.value)
 
+    def submit_many(self, pqs: Sequence[PreparedGroupby]) -> list[int]:
+        """Submits a burst of queries in one call (bolt_server_submit_batch),
+        so the lanes see it whole and form full batches."""
+        n = len(pqs)
+        qs = (_abi.Query * max(n, 1))(*[_abi.Query(pq.desc, pq.out, pq.rows[0], pq.rows[1], 0) for pq in pqs])
+        ts = (C.c_uint64 * max(n, 1))()
+        st = self._lib.bolt_server_submit_batch(self._h, qs, n, ts)
+        if st != _abi.OK:
+            raise _ERRORS.get(st, BoltError)(f"bolt_server_submit_batch failed: {_abi.STATUS_NAMES[st]}", st)
+        out = []
+        for i, pq in enumerate(pqs):
+            t = int(ts[i])
+            # The Query structs live in `qs`, which every pending entry keeps alive.
+            self._pending[t] = (pq, qs[i], qs)
+            out.append(t)
+        return out
+
     def wait(self, ticket: int) -> tuple[GroupbyResult, float]:
         lat = C.c_double(0.0)
         st = self._lib.bolt_server_wait(self._h, ticket, C.byref(lat))
-        pq, q = self._pending.pop(ticket)
+        pq, q = self._pending.pop(ticket)[:2]
         if st != _abi.OK:
             raise _ERRORS.get(st, BoltError)(f"query {ticket} failed: {_abi.STATUS_NAMES[st]}", st)
         pq.out.n_groups = q.out.n_groups

@@ -126,6 +126,7 @@ SIGNATURES = {
     "bolt_graph_destroy": (None, [C.c_void_p]),
     "bolt_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "bolt_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+    "bolt_server_submit_batch": (C.c_int, [C.c_void_p, C.POINTER(Query), C.c_int32, C.POINTER(C.c_uint64)]),
     "bolt_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_double)]),
     "bolt_server_destroy": (None, [C.c_void_p]),
 }

@@ -211,6 +211,40 @@ extern "C" bolt_status bolt_server_submit(bolt_server* srv, bolt_query* q, uint6
     return BOLT_OK;
 }
 
+// A burst of queries enqueued under one lock and announced once, so the
+// lanes see it whole and form full batches (one call per query lets the
+// lanes drain the queue as the queries trickle in, a few at a time).
+extern "C" bolt_status bolt_server_submit_batch(bolt_server* srv, bolt_query* qs, int32_t n, uint64_t* tickets) {
+    if (!srv || n < 0 || (n > 0 && (!qs || !tickets))) return BOLT_ERR_INVALID;
+    std::vector<Req*> rs((size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+        Req* r = new Req();
+        r->q = &qs[i];
+        r->footprint = bolt_groupby_footprint(&qs[i].desc, query_rows(&qs[i]));
+        if (r->footprint > srv->lane_budget) {
+            delete r;
+            for (int32_t j = 0; j < i; ++j) delete rs[(size_t)j];
+            return BOLT_ERR_CAPACITY;
+        }
+        rs[(size_t)i] = r;
+    }
+    const auto now = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        for (int32_t i = 0; i < n; ++i) {
+            Req* r = rs[(size_t)i];
+            r->t_submit = now;
+            r->ticket = srv->next_ticket++;
+            srv->reqs[r->ticket] = r;
+            srv->queue.push_back(r);
+            if (query_rows(r->q) >= BIG_QUERY_ROWS) ++srv->n_big;
+            tickets[i] = r->ticket;
+        }
+    }
+    srv->cv_work.notify_all();
+    return BOLT_OK;
+}
+
 extern "C" bolt_status bolt_server_wait(bolt_server* srv, uint64_t ticket, double* latency_us) {
     if (!srv) return BOLT_ERR_INVALID;
     std::unique_lock<std::mutex> lk(srv->mu);

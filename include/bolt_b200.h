@@ -372,6 +372,12 @@ bolt_status bolt_server_create(const bolt_server_config* cfg, bolt_server** out)
 /* Submits a query; `q` and every buffer it names must stay alive until
  * bolt_server_wait returns for the ticket. */
 bolt_status bolt_server_submit(bolt_server* srv, bolt_query* q, uint64_t* ticket);
+/* Submits n queries at once (no counterpart in the reference, which runs one
+ * query at a time): tickets[i] receives query i's ticket. The burst is
+ * enqueued under one lock and announced once, so the lanes form full batches
+ * from it. All or none: BOLT_ERR_CAPACITY when any query's footprint exceeds
+ * a lane's share of HBM. Same lifetime rule as bolt_server_submit. */
+bolt_status bolt_server_submit_batch(bolt_server* srv, bolt_query* qs, int32_t n, uint64_t* tickets);
 /* Blocks until the ticket completes; latency_us receives submit -> done. */
 bolt_status bolt_server_wait(bolt_server* srv, uint64_t ticket, double* latency_us);
 void        bolt_server_destroy(bolt_server* srv);

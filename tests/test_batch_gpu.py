@@ -141,23 +141,31 @@ def test_batch_graph_replay(bolt, engine, oracle):
         g.close()
 
 
-@pytest.mark.parametrize("n,n_q,lanes", [(300_000, 60, 2), (12_000_000, 24, 4)])
-def test_server_mix_equals_alone(bolt, engine, oracle, n, n_q, lanes):
+@pytest.mark.parametrize("n,n_q,lanes,burst", [(300_000, 60, 2, False), (12_000_000, 24, 4, False),
+                                               (300_000, 200, 4, True), (12_000_000, 40, 3, True)])
+def test_server_mix_equals_alone(bolt, engine, oracle, n, n_q, lanes, burst):
     """Served results equal the query run alone. The larger table gives
-    queries above the size that is admitted alone, and four lanes run
-    different kernels and shared-memory sizes concurrently."""
+    queries above the size that is admitted alone, and several lanes run
+    different kernels and shared-memory sizes concurrently. `burst` submits
+    all queries in one bolt_server_submit_batch call, so lanes form full
+    batches."""
     t, dts, dev = make_table(bolt, n, 5)
     specs = query_specs(n, n_q, 6)
     kdev, khost = keyed_columns(bolt, t, dts, specs)
     srv = bolt.Server(0, scratch_bytes=4 << 30, max_batch=16, n_lanes=lanes)
     try:
-        tickets = []
+        tickets, pqs = [], []
         for s in specs:
             kname = f"{s['key']}_{s['card']}"
             table = {kname: kdev[kname], s["val"]: dev[s["val"]], "f": dev["f"]}
             pq = engine.prepare_groupby(table, [kname], [("sum", s["val"]), ("count_star", None)],
                                         [("f", "<", s["t"])], groups_hint=s["card"], rows=(s["begin"], s["end"]))
-            tickets.append((srv.submit(pq), s, kname))
+            pqs.append((pq, s, kname))
+        if burst:
+            ts = srv.submit_many([pq for pq, _, _ in pqs])
+            tickets = [(t, s, kname) for t, (_, s, kname) in zip(ts, pqs)]
+        else:
+            tickets = [(srv.submit(pq), s, kname) for pq, s, kname in pqs]
         lat = []
         for ticket, s, kname in tickets:
             r, us = srv.wait(ticket)
