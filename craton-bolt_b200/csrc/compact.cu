@@ -458,6 +458,7 @@ template <int ITEMS, bool VEC>
 __global__ void __launch_bounds__(CP_BLOCK) compact_count_kernel(const __grid_constant__ CpArgs a) {
     constexpr int TILE = CP_BLOCK * ITEMS;
     constexpr int R = ITEMS * CC_GROUP;  // rows per thread per step
+    static_assert(!VEC || CP_BLOCK * 16 == CC_GROUP * TILE, "vectorised count: 16 rows per thread cover the group");
     __shared__ uint32_t wcnt[CC_GROUP][CP_NW];
     const CompactSpec& sp = a.sp;
     const uint64_t n = sp.n;
