@@ -186,6 +186,32 @@ def test_groupby_f64_sum_close_to_exact(bolt, engine, oracle):
     assert np.all(np.abs(got - acc) <= ulp + 1e-15)
 
 
+@pytest.mark.parametrize("tier", ["default", "force_global"])
+@pytest.mark.parametrize("with_out_of_window", [False, True])
+def test_groupby_f64_sum_window_edges(bolt, engine, oracle, tier, with_out_of_window):
+    """f64 SUM / AVG at the edges of the fixed-point window: magnitudes just
+    below 2^32 (the global table's signed high word then carries its largest
+    sums), tiny and subnormal values, signed zeros and cancelling signs, in
+    both tiers. With a value of magnitude 2^32 the call falls back to f64
+    atomics and still meets the tolerance."""
+    rng = np.random.default_rng(31)
+    n = 200_000
+    pool = np.array([4294967295.5, -4294967295.5, 4294967296.0 - 2.0 ** -20, -(4294967296.0 - 2.0 ** -20),
+                     1e-300, -1e-300, 5e-324, 0.0, -0.0, 1.0, -1.0, 123456.789], dtype=np.float64)
+    v = pool[rng.integers(0, len(pool), n)]
+    if with_out_of_window:
+        # The fallback's f64 atomics round in arrival order: non-negative
+        # values keep every partial sum below the final one, so its rounding
+        # error stays within the tolerance whatever the order.
+        v = np.abs(v)
+        v[::997] = 4294967296.0
+    k = rng.integers(0, 64, n).astype(np.int32)
+    cols = {"k": (k, None, "i32", 0), "v": (v, None, "f64", 0)}
+    aggs = [("sum", "v"), ("avg", "v"), ("count_star", None)]
+    flags = bolt.FLAG_FORCE_GLOBAL if tier == "force_global" else 0
+    run_both(bolt, engine, oracle, cols, ["k"], aggs, hint=64, flags=flags)
+
+
 def test_groupby_null_keys_and_values(bolt, engine, oracle):
     rng = np.random.default_rng(3)
     n = 100_000
