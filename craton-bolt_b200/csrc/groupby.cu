@@ -1577,7 +1577,12 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     // Untuned default: the register kernel for small inputs, the staged
     // kernel (2 chunks per consumer warp) from 4M rows, where its pipeline
     // fills.
-    bolt_ctx::GbTune tn{512, 1, 0, 1, 4, n >= (1ull << 22) ? 2 : 0, 0.0};
+    // Shared-tier admission cap in eighths of the table: half full when the
+    // expected groups fit in it; 3/8 when they outnumber it, so keys that miss
+    // meet an empty slot sooner (shorter divergent probe loops; measured
+    // 3.05 -> 2.95 ms at 100M rows and 3.28M groups).
+    const int fill = (hint && hint <= 1024) ? 4 : 3;
+    bolt_ctx::GbTune tn{512, 1, 0, 1, fill, n >= (1ull << 22) ? 2 : 0, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
@@ -2533,7 +2538,7 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
         for (int smem_shift : {0, 1})
             for (int warp_agg : {0, 1})
                 for (int load_shift : {0, 1, 2})
-                    for (int smem_fill : {4, 6}) cands.push_back({512, smem_shift, warp_agg, load_shift, smem_fill, staged, 0.0});
+                    for (int smem_fill : {2, 3, 4, 6}) cands.push_back({512, smem_shift, warp_agg, load_shift, smem_fill, staged, 0.0});
     bolt_ctx::GbTune best{512, 1, 0, 1, 4, 0, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
