@@ -611,7 +611,9 @@ def w_compact(c: Ctx):
 
     ms, launches, kms, clocks = c.timed(step, a.steps, a.warmup)
     alg = a.rows * FILTERED_BYTES * 1.5  # read all columns, write the ~50% kept
-    return base_line(c, ms, a.rows, alg, kms, "compact_kernel", "compact",
+    kernel = ("compact_count_kernel + compact_scan_kernel + compact_bulk_kernel (two-pass form)"
+              if a.rows >= (1 << 22) else "compact_bulk_kernel")
+    return base_line(c, ms, a.rows, alg, kms, kernel, "compact",
                      {"workload": "WHERE f < 50 compaction of 5 columns (28 B/row), 100M rows", "rows": a.rows,
                       "l2": "inputs larger than L2"}, launches, clocks, "mixed")
 
