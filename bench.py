@@ -321,16 +321,16 @@ def base_line(c: Ctx, ms: float, rows_per_step: float, alg_bytes: float, kms, ke
 FILTERED_AGGS = [("sum", "vd"), ("avg", "vd"), ("count_star", None), ("min", "vi"), ("max", "vi")]
 FILTERED_DT = {"a": "i32", "b": "i32", "f": "i32", "vd": "f64", "vi": "i64"}
 FILTERED_BYTES = 4 + 4 + 4 + 8 + 8
+FILTERED_WORKLOAD = ("filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) ranks, "
+                     "WHERE f < 50, SUM/AVG(vd f64), COUNT(*), MIN/MAX(vi i64)")
 
 
 def gen_filtered(n: int, device: str | None):
     dg = datagen()
     cdf = dg.zipf_cdf(10_000_000, 1.1)
     if device is not None:
-        ranks = dg.zipf_ranks_torch(cdf, 2, n, device)
-    else:
-        ranks = dg.zipf_ranks(cdf, dg.unit_f64(dg.uniform_u64(2, 10, n)))
-    return dg.groupby_filtered(n, seed=2, ranks=ranks)
+        return dg.groupby_filtered(n, seed=2, ranks=dg.zipf_ranks_torch(cdf, 2, n, device))
+    return dg.groupby_filtered(n, seed=2, cdf=cdf)
 
 
 class PreparedCall:
@@ -365,12 +365,18 @@ def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
     return "gb_staged_kernel" if staged else "gb_agg_kernel"
 
 
-def cpu_rows_per_s_groupby(table_np: dict, dts: dict, group_by, aggs, where, n_sample: int):
+def cpu_rows_per_s_groupby(table_np: dict, dts: dict, group_by, aggs, where, n_sample: int, runs: int = 5):
+    """Rows/s of the oracle's 1-thread GROUP BY on the first n_sample rows:
+    the median of `runs` timed runs after one warm-up run."""
     orc = oracle_mod()
     host = {k: orc.HostCol(np.ascontiguousarray(v[:n_sample]), dts[k]) for k, v in table_np.items()}
-    t0 = time.perf_counter()
     orc.groupby(host, group_by, aggs, where=where)
-    return n_sample / (time.perf_counter() - t0)
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        orc.groupby(host, group_by, aggs, where=where)
+        times.append(time.perf_counter() - t0)
+    return n_sample / statistics.median(times)
 
 
 def w_groupby_filtered(c: Ctx):
@@ -403,8 +409,7 @@ def w_groupby_filtered(c: Ctx):
     progress(f"timed: {ms / a.steps:.3f} ms/step, {n_groups} groups")
     alg = a.rows * FILTERED_BYTES
     line = base_line(c, ms, a.rows, alg, kms, kernel, "groupby_filtered",
-                     {"workload": "filtered two-key GROUP BY: 100M rows, (a,b) int32 pairs of 10M Zipf(1.1) ranks, "
-                                  "WHERE f < 50, SUM/AVG(vd f64), COUNT(*), MIN/MAX(vi i64)",
+                     {"workload": FILTERED_WORKLOAD,
                       "rows": a.rows, "groups": n_groups, "groups_hint": a.groups_hint,
                       "autotuned": tuned,
                       "l2": "inputs (2.8 GB) larger than L2 (126 MB); no flush needed"},
@@ -428,7 +433,7 @@ def w_groupby_filtered(c: Ctx):
         rps = cpu_rows_per_s_groupby(data, FILTERED_DT, ["a", "b"], FILTERED_AGGS, [("f", "<", 50)], ns)
         line["cpu_baseline"] = {"value": rps, "unit": "rows/s", "cores": 1, "kind": "port",
                                 "sample": f"first {ns} rows of the workload; CPU restatement of the reference's "
-                                          "host GROUP BY (oracle), 1 thread"}
+                                          "host GROUP BY (oracle), 1 thread; median of 5 runs after 1 warm-up"}
     return line
 
 
@@ -770,42 +775,40 @@ WORKLOADS = {"groupby_filtered": w_groupby_filtered, "groupby_plain": w_groupby_
 # Reference arm
 # ---------------------------------------------------------------------------
 def run_reference(args):
-    """CPU restatement of the reference's host GROUP BY path, timed per step
-    on a bounded sample of the workload's rows."""
-    from concurrent.futures import ThreadPoolExecutor
-
-    n_sample = args.reference_rows
-    data = gen_filtered(n_sample, None)
+    """The reference's host GROUP BY path (restated in C: the reference is
+    Rust and cannot be built here) over the full workload, every step, on
+    every host thread: rows are range-partitioned by key and each partition
+    is folded in row order by one thread, so the result equals the
+    sequential fold's. Partitioning, folding, the per-partition sort and the
+    output assembly are all timed."""
+    progress(f"reference arm: generating {args.rows} rows on the host")
+    data = gen_filtered(args.rows, None)
     orc = oracle_mod()
     host = {k: orc.HostCol(np.ascontiguousarray(v), FILTERED_DT[k]) for k, v in data.items()}
-    # Every host thread runs the sample's GROUP BY at once (the oracle's C
-    # code runs outside the GIL), as a host engine would run one partition
-    # per core; merging the per-thread partial groups is not timed.
-    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-
-    def one(_):
-        orc.groupby(host, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)])
-
-    times = []
-    with ThreadPoolExecutor(max_workers=threads) as pool:
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            list(pool.map(one, range(threads)))
-            if i >= args.warmup:
-                times.append(time.perf_counter() - t0)
+    threads = orc.host_threads()
+    times, groups = [], None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        r = orc.groupby(host, ["a", "b"], FILTERED_AGGS, where=[("f", "<", 50)], threads=threads)
+        dt = time.perf_counter() - t0
+        groups = r["n_groups"]
+        del r
+        if i >= args.warmup:
+            times.append(dt)
+        progress(f"reference step {i}: {dt * 1e3:.1f} ms")
     total = sum(times)
-    value = n_sample * threads * len(times) / total
+    value = args.rows * len(times) / total
     line = {"metric": METRIC, "value": value, "unit": "rows/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "ms_per_step_median": 1e3 * statistics.median(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64",
-            "data": "synthetic (seeded, same generator as the GPU arm)",
-            "config": {"workload": "filtered two-key GROUP BY (Zipf(1.1) pairs, f < 50)",
-                       "rows_per_step": n_sample * threads, "rows_full": args.rows,
-                       "parallelism": f"host, {threads} threads"},
+            "data": "synthetic (seeded splitmix64 generator; same rows as the GPU arm)",
+            "config": {"workload": FILTERED_WORKLOAD, "rows": args.rows, "groups": groups,
+                       "rows_per_step": args.rows, "parallelism": f"host, {threads} threads"},
             "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
-                             "sample": f"first {n_sample} rows of the workload, GROUP BY run by each of {threads} "
-                                       "host threads at once per step; the reference is Rust (no cargo here), "
-                                       "timed as its C restatement (one HashMap pass per thread, merge not timed)"},
+                             "sample": f"all {args.rows} rows of the workload every step; the reference's host "
+                                       "GROUP BY (HashMap fold in row order, sorted output) restated in C, on "
+                                       f"{threads} threads (key-range partitions), everything timed"},
             "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -832,7 +835,6 @@ def main():
     ap.add_argument("--scratch-gb", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-rows", type=int, default=10_000_000)
-    ap.add_argument("--reference-rows", type=int, default=2_000_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the GROUP BY autotuner")

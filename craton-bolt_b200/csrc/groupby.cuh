@@ -156,6 +156,15 @@ struct GbPlan {
     ull* words = nullptr;  // device: [0] occupancy, [1] non-NULL groups, [2] groups, [3] status
     uint64_t shape = 0;    // autotuning key of the query shape
     bolt_ctx::GbTune tune{512, 1, 0, 1, 4, 0, 0.0};
+    uint64_t groups_hint = 0;  // expected groups (the caller's hint, at most the rows)
+    // Hash-partitioned tier (groupby_part.cu): shared-table size of its
+    // streaming kernel (log2; 0 = default), 32-row chunks per consumer warp
+    // per tile, the partition count used (log2), and whether the finalize
+    // finds the groups already compacted with their sort keys.
+    int32_t part_hot_log2 = 0;
+    int32_t part_chunks = 1;
+    int32_t part_pbits = 0;
+    bool precompacted = false;
 };
 
 // Key of a query shape for the autotuning cache: key / predicate / state

@@ -8,6 +8,9 @@ reference's h2o-style benchmark shapes.
 
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 
 M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
@@ -55,8 +58,34 @@ def groupby_small(n: int = 1_000_000, seed: int = 1, n_keys: int = 1024):
 # ---------------------------------------------------------------------------
 # Filtered two-key GROUP BY: (a, b) int32 pairs of Zipf(s) ranks, f < 50 filter
 # ---------------------------------------------------------------------------
+CHUNK = 1 << 22
+
+
+def _threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def _chunked(n: int, fn) -> None:
+    """Runs fn(start, stop) over row chunks on every host thread (numpy's
+    ufuncs and searchsorted release the GIL). The generators are pure
+    functions of the row index, so the chunking does not change any value."""
+    spans = [(s, min(n, s + CHUNK)) for s in range(0, n, CHUNK)]
+    if len(spans) <= 1:
+        for s, e in spans:
+            fn(s, e)
+        return
+    with ThreadPoolExecutor(max_workers=min(_threads(), len(spans))) as pool:
+        for f in [pool.submit(fn, s, e) for s, e in spans]:
+            f.result()
+
+
 def zipf_cdf(n_ranks: int, s: float) -> np.ndarray:
-    w = np.arange(1, n_ranks + 1, dtype=np.float64) ** (-s)
+    w = np.empty(n_ranks, dtype=np.float64)
+
+    def part(a, b):
+        w[a:b] = np.arange(a + 1, b + 1, dtype=np.float64) ** (-s)
+
+    _chunked(n_ranks, part)
     c = np.cumsum(w)
     return c / c[-1]
 
@@ -81,12 +110,19 @@ def groupby_filtered(n: int, seed: int = 2, n_pairs: int = 10_000_000, s: float 
     vi (int64 uniform over the full range)."""
     if ranks is None:
         cdf = zipf_cdf(n_pairs, s) if cdf is None else cdf
-        ranks = zipf_ranks(cdf, unit_f64(uniform_u64(seed, 10, n)))
-    a, b = pair_of_rank(ranks, seed)
-    f = ((uniform_u64(seed, 11, n) >> np.uint64(32)) % np.uint64(100)).astype(np.int32)
-    vd = normal_f64(seed, 12, n, 1e3)
-    vi = uniform_u64(seed, 14, n).view(np.int64)
-    return {"a": a, "b": b, "f": f, "vd": vd, "vi": vi}
+    out = {"a": np.empty(n, np.int32), "b": np.empty(n, np.int32), "f": np.empty(n, np.int32),
+           "vd": np.empty(n, np.float64), "vi": np.empty(n, np.int64)}
+
+    def part(s0, s1):
+        m = s1 - s0
+        rk = ranks[s0:s1] if ranks is not None else zipf_ranks(cdf, unit_f64(uniform_u64(seed, 10, m, s0)))
+        out["a"][s0:s1], out["b"][s0:s1] = pair_of_rank(rk, seed)
+        out["f"][s0:s1] = ((uniform_u64(seed, 11, m, s0) >> np.uint64(32)) % np.uint64(100)).astype(np.int32)
+        out["vd"][s0:s1] = normal_f64(seed, 12, m, 1e3, s0)
+        out["vi"][s0:s1] = uniform_u64(seed, 14, m, s0).view(np.int64)
+
+    _chunked(n, part)
+    return out
 
 
 def zipf_ranks_torch(cdf: np.ndarray, seed: int, n: int, device: str, chunk: int = 1 << 25):
@@ -95,10 +131,16 @@ def zipf_ranks_torch(cdf: np.ndarray, seed: int, n: int, device: str, chunk: int
     import torch
 
     c = torch.from_numpy(cdf).to(device)
+    uh = np.empty(n, np.float64)
+
+    def part(a, b):
+        uh[a:b] = unit_f64(uniform_u64(seed, 10, b - a, a))
+
+    _chunked(n, part)
     out = torch.empty(n, dtype=torch.int64)
     for s0 in range(0, n, chunk):
         m = min(chunk, n - s0)
-        u = torch.from_numpy(unit_f64(uniform_u64(seed, 10, m, s0))).to(device)
+        u = torch.from_numpy(uh[s0:s0 + m]).to(device)
         r = torch.searchsorted(c, u, right=True) + 1
         out[s0:s0 + m] = torch.clamp(r, max=len(cdf)).cpu()
     return out.numpy()

@@ -93,6 +93,9 @@ typedef struct bolt_ctx bolt_ctx;
 #define BOLT_FLAG_KERNEL_REGS  0x20u /* GROUP BY: aggregate with the register-tile kernel; compaction: per-element
                                        copies instead of bulk-staged tiles (testing) */
 #define BOLT_FLAG_KERNEL_STAGED 0x40u /* GROUP BY: aggregate with the staged kernel where it applies (testing) */
+#define BOLT_FLAG_NO_PART      0x80u /* GROUP BY: never use the hash-partitioned tier (global hash table instead) */
+#define BOLT_FLAG_FORCE_PART   0x100u /* GROUP BY: use the hash-partitioned tier wherever it applies, whatever the
+                                        groups hint (testing) */
 
 /* ------------------------------------------------------------------------ */
 /* Context: device, scratch arena, tuning cache, status word, last error.   */
@@ -215,14 +218,20 @@ bolt_status bolt_groupby_host(bolt_ctx* ctx, const bolt_groupby_desc* desc,
  * engine whose own pool owns all of HBM, or a latency-critical loop where an
  * allocation would synchronise the device) and so cannot hold a bolt_ctx.
  * Same semantics and outputs as bolt_groupby (device columns in, device
- * columns out), for at most 6144 groups (an 8192-slot table). Its scratch is
- * one fixed 2 MiB device array inside this library, held by every GPU that
- * loads it until the process exits. The first call on a device (with that
- * device current) resolves the array's address: make it before any stream
- * capture. Calls share the array and clear it on entry, so calls that
- * overlap on the GPU race: serialise them. The call synchronises `stream`.
- * More groups -> BOLT_ERR_CAPACITY; `err` (nullable, err_cap bytes) receives
- * the message of a failure. */
+ * columns out), for at most 6144 groups: the table starts at the size the
+ * groups hint asks for and grows, up to 8192 slots, when the groups outnumber
+ * the hint. Its scratch is one fixed 2 MiB device array inside this library,
+ * held by every GPU that loads it until the process exits. The first call on
+ * each device (with that device current) resolves the array's address with
+ * cudaGetSymbolAddress: make that first call before any stream capture
+ * begins. Calls share the array and clear it on entry, so calls that overlap
+ * on the GPU race: serialise them. Every call waits for its own work on
+ * `stream` before it returns (it reads the group count and status back).
+ * Returns: more than 6144 groups, or out_cap below the group count ->
+ * BOLT_ERR_CAPACITY; a SUM(Int64) whose inputs are large enough to need the
+ * row-order overflow check (bolt_groupby runs it with scratch it allocates)
+ * -> BOLT_DECLINE. `err` (nullable, err_cap bytes) receives the message of a
+ * failure. */
 bolt_status bolt_groupby_noalloc(const bolt_groupby_desc* desc, bolt_groupby_out* out,
                                  bolt_stream stream, char* err, int32_t err_cap);
 

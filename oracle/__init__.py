@@ -84,10 +84,19 @@ def _cols(table: dict):
     return names, arr
 
 
-def groupby(table: dict, group_by, aggs, where=()):
+def host_threads() -> int:
+    """Host threads this process may run on."""
+    import os
+
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def groupby(table: dict, group_by, aggs, where=(), threads: int = 1):
     """GROUP BY restated from groupby.rs:295-833. Returns dict with 'keys'
     (packed i64), 'key_null', per-aggregate 'vals' / 'valid' and 'accurate'
-    (compensated f64 sums), 'n_groups'."""
+    (compensated f64 sums), 'n_groups'. `threads` > 1 runs the same fold on
+    that many host threads (key-range partitions, each folded in row order):
+    identical results."""
     names, arr = _cols(table)
     n = len(table[group_by[0]].data)
     kidx = (C.c_int32 * len(group_by))(*[names.index(k) for k in group_by])
@@ -124,11 +133,16 @@ def groupby(table: dict, group_by, aggs, where=()):
     accptr = (C.c_void_p * len(aggs))(*[v.ctypes.data for v in accs])
     ng = C.c_uint64(0)
     err = C.create_string_buffer(256)
-    f = lib().orc_groupby
+    args = [C.c_uint64(n), arr, len(names), kidx, len(group_by), parr, len(preds), sarr, len(specs),
+            keys.ctypes.data_as(C.c_void_p), knull.ctypes.data_as(C.c_void_p), vptr, valptr, accptr,
+            C.c_uint64(cap), C.byref(ng), err, 256]
+    if threads > 1:
+        f = lib().orc_groupby_par
+        args.append(C.c_int32(int(threads)))
+    else:
+        f = lib().orc_groupby
     f.restype = C.c_int
-    st = f(C.c_uint64(n), arr, len(names), kidx, len(group_by), parr, len(preds), sarr, len(specs),
-           keys.ctypes.data_as(C.c_void_p), knull.ctypes.data_as(C.c_void_p), vptr, valptr, accptr,
-           C.c_uint64(cap), C.byref(ng), err, 256)
+    st = f(*args)
     if st != OK:
         raise OracleError(st, err.value.decode() or f"oracle status {st}")
     g = int(ng.value)

@@ -25,6 +25,7 @@
 #include "bolt_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -223,6 +224,206 @@ static int cmp_grp(const void* x, const void* y) {
     return 0;
 }
 
+/* One GROUP BY fold in progress: the key map, the groups in first-seen
+ * order and their accumulators. */
+typedef struct {
+    const orc_col* cols;
+    const int32_t* key_cols;
+    int32_t n_keys;
+    const orc_agg* aggs;
+    int32_t n_aggs;
+    omap m;
+    uint64_t ng, gcap;
+    grp_t* groups;
+    acc_t* acc;
+    int64_t null_group;
+    int status;
+    char err[256];
+} gb_state;
+
+static int gbs_init(gb_state* s, const orc_col* cols, const int32_t* key_cols, int32_t n_keys,
+                    const orc_agg* aggs, int32_t n_aggs, uint64_t expect) {
+    memset(s, 0, sizeof *s);
+    s->cols = cols; s->key_cols = key_cols; s->n_keys = n_keys; s->aggs = aggs; s->n_aggs = n_aggs;
+    s->null_group = -1;
+    s->gcap = expect < 1024 ? 1024 : expect;
+    if (omap_init(&s->m, s->gcap)) return -1;
+    s->groups = (grp_t*)malloc(s->gcap * sizeof(grp_t));
+    s->acc = (acc_t*)calloc(s->gcap * (uint64_t)n_aggs, sizeof(acc_t));
+    return (s->groups && s->acc) ? 0 : -1;
+}
+
+static void gbs_free(gb_state* s) {
+    omap_free(&s->m);
+    free(s->groups);
+    free(s->acc);
+}
+
+/* Folds row r (it passed the WHERE conjunction; a multi-column key with a
+ * NULL part was already dropped, groupby.rs:600-615) into its group. The
+ * accumulators follow the reference's host fold in row order: checked i64
+ * SUM (checked_group_sum, groupby.rs:1775-1798), sequential f64 SUM,
+ * checked i128 Decimal SUM (aggregate.rs:1220). */
+static void gbs_fold_row(gb_state* st, uint64_t r, int key_null) {
+    const orc_col* cols = st->cols;
+    uint32_t g;
+    if (key_null) {
+        if (st->null_group < 0) {
+            st->null_group = (int64_t)st->ng;
+            goto new_group;
+        }
+        g = (uint32_t)st->null_group;
+    } else {
+        int ins;
+        int64_t key = orc_pack_key(cols, st->key_cols, st->n_keys, r);
+        if (st->ng * 2 >= st->m.cap && omap_grow(&st->m)) { st->status = ORC_CAPACITY; return; }
+        g = omap_get(&st->m, (uint64_t)key, (uint32_t)st->ng, &ins);
+        if (ins) goto new_group;
+    }
+    goto have_group;
+new_group:
+    if (st->ng == st->gcap) {
+        uint64_t nc = st->gcap * 2;
+        st->groups = (grp_t*)realloc(st->groups, nc * sizeof(grp_t));
+        st->acc = (acc_t*)realloc(st->acc, nc * (uint64_t)st->n_aggs * sizeof(acc_t));
+        memset(st->acc + st->gcap * (uint64_t)st->n_aggs, 0, (nc - st->gcap) * (uint64_t)st->n_aggs * sizeof(acc_t));
+        st->gcap = nc;
+    }
+    g = (uint32_t)st->ng++;
+    st->groups[g].is_null = key_null;
+    st->groups[g].key = key_null ? INT64_MAX : orc_pack_key(cols, st->key_cols, st->n_keys, r);
+    st->groups[g].row_first = (uint32_t)r;
+have_group:
+    for (int32_t a = 0; a < st->n_aggs; ++a) {
+        acc_t* s = &st->acc[(uint64_t)g * st->n_aggs + a];
+        int op = st->aggs[a].op;
+        if (op == ORC_COUNT_STAR) { s->cnt++; continue; }
+        const orc_col* c = &cols[st->aggs[a].input_col];
+        if (!is_valid(c->validity, r)) continue;
+        if (op == ORC_COUNT) { s->cnt++; continue; }
+        if (op == ORC_MIN || op == ORC_MAX) {
+            uint64_t k = mm_key(c, r);
+            if (s->cnt == 0) { s->mnk = s->mxk = k; }
+            else { if (k < s->mnk) s->mnk = k; if (k > s->mxk) s->mxk = k; }
+            s->cnt++;
+            continue;
+        }
+        /* SUM / AVG */
+        s->cnt++;
+        if (is_float(c->dtype)) {
+            double v = col_f64(c, r);
+            s->fsum += v;
+            double t = s->csum + v;
+            if (fabs(s->csum) >= fabs(v)) s->comp += (s->csum - t) + v;
+            else s->comp += (v - t) + s->csum;
+            s->csum = t;
+        } else if (c->dtype == ORC_DEC128) {
+            i128 v = col_i128(c, r), out;
+            if (__builtin_add_overflow(s->isum, v, &out)) {
+                if (st->status == ORC_OK) {
+                    snprintf(st->err, sizeof st->err,
+                             "SUM(Decimal128) precision overflow: accumulator exceeds i128 range");
+                    st->status = ORC_OVERFLOW;
+                }
+            } else s->isum = out;
+        } else {
+            int64_t v = col_i64(c, r);
+            if (c->dtype == ORC_I64 && op == ORC_SUM) {
+                /* checked_group_sum (groupby.rs:1775): checked i64 add in row order */
+                int64_t cur = (int64_t)s->isum, out;
+                if (__builtin_add_overflow(cur, v, &out)) {
+                    if (st->status == ORC_OK) {
+                        snprintf(st->err, sizeof st->err, "SUM(integer) overflow: accumulator exceeds i64 range");
+                        st->status = ORC_OVERFLOW;
+                    }
+                } else s->isum = out;
+            } else {
+                s->isum += v;
+            }
+        }
+    }
+}
+
+/* Group indices in output order: packed key ascending as i64, NULL group
+ * last (groupby.rs:789-800). */
+static uint32_t* gbs_order(const gb_state* st) {
+    const uint64_t ng = st->ng;
+    uint32_t* order = (uint32_t*)malloc((ng ? ng : 1) * sizeof(uint32_t));
+    grp_t* sorted = (grp_t*)malloc((ng ? ng : 1) * sizeof(grp_t));
+    for (uint64_t g = 0; g < ng; ++g) { sorted[g] = st->groups[g]; sorted[g].row_first = (uint32_t)g; }
+    qsort(sorted, ng, sizeof(grp_t), cmp_grp);
+    for (uint64_t g = 0; g < ng; ++g) order[g] = sorted[g].row_first;
+    free(sorted);
+    return order;
+}
+
+/* Writes the groups of `order` to output rows [o_base, o_base + ng). */
+static void gbs_emit(const gb_state* st, const uint32_t* order, uint64_t o_base,
+                     int64_t* out_keys, uint8_t* out_key_null,
+                     void** out_vals, uint8_t** out_valid, double** out_accurate) {
+    const orc_col* cols = st->cols;
+    for (uint64_t i = 0; i < st->ng; ++i) {
+        const uint64_t o = o_base + i;
+        uint32_t g = order[i];
+        out_keys[o] = st->groups[g].is_null ? 0 : st->groups[g].key;
+        out_key_null[o] = (uint8_t)st->groups[g].is_null;
+        for (int32_t a = 0; a < st->n_aggs; ++a) {
+            const acc_t* s = &st->acc[(uint64_t)g * st->n_aggs + a];
+            int op = st->aggs[a].op;
+            uint8_t valid = 1;
+            const orc_col* c = op == ORC_COUNT_STAR ? NULL : &cols[st->aggs[a].input_col];
+            if (op == ORC_COUNT_STAR || op == ORC_COUNT) {
+                ((int64_t*)out_vals[a])[o] = s->cnt;
+            } else if (op == ORC_MIN || op == ORC_MAX) {
+                valid = s->cnt > 0;
+                uint64_t k = op == ORC_MIN ? s->mnk : s->mxk;
+                if (is_float(c->dtype)) ((double*)out_vals[a])[o] = valid ? mm_key_to_f64(k) : 0.0;
+                else ((int64_t*)out_vals[a])[o] = valid ? (int64_t)(k ^ 0x8000000000000000ull) : 0;
+            } else if (op == ORC_SUM) {
+                valid = s->cnt > 0;
+                if (is_float(c->dtype)) {
+                    ((double*)out_vals[a])[o] = valid ? s->fsum : 0.0;
+                    if (out_accurate && out_accurate[a]) out_accurate[a][o] = s->csum + s->comp;
+                } else if (c->dtype == ORC_DEC128) {
+                    i128 v = valid ? s->isum : 0;
+                    ((uint64_t*)out_vals[a])[2 * o] = (uint64_t)v;
+                    ((uint64_t*)out_vals[a])[2 * o + 1] = (uint64_t)((unsigned __int128)v >> 64);
+                } else {
+                    ((int64_t*)out_vals[a])[o] = valid ? (int64_t)s->isum : 0;
+                }
+            } else { /* AVG = (sum f64) / count (groupby.rs:2877-2885) */
+                valid = s->cnt > 0;
+                double sum = is_float(c->dtype) ? s->fsum : (double)s->isum;
+                ((double*)out_vals[a])[o] = valid ? sum / (double)s->cnt : 0.0;
+                if (out_accurate && out_accurate[a])
+                    out_accurate[a][o] = valid ? (is_float(c->dtype) ? (s->csum + s->comp) : (double)s->isum) / (double)s->cnt : 0.0;
+            }
+            if (out_valid && out_valid[a]) out_valid[a][o] = valid;
+        }
+    }
+}
+
+static int gb_check_aggs(const orc_col* cols, const orc_agg* aggs, int32_t n_aggs) {
+    for (int32_t a = 0; a < n_aggs; ++a) {
+        int op = aggs[a].op;
+        if (op == ORC_COUNT_STAR) continue;
+        const orc_col* c = &cols[aggs[a].input_col];
+        if ((op == ORC_SUM || op == ORC_AVG) && c->dtype == ORC_F32) return ORC_DECLINE;
+        if ((op == ORC_MIN || op == ORC_MAX || op == ORC_AVG) && c->dtype == ORC_DEC128)
+            return ORC_DECLINE;
+    }
+    return ORC_OK;
+}
+
+/* Key NULL-ness of row r; -1 when the row is dropped (multi-column key with a
+ * NULL part). */
+static inline int gb_key_null(const orc_col* cols, const int32_t* key_cols, int32_t n_keys, uint64_t r) {
+    int key_null = 0;
+    for (int32_t k = 0; k < n_keys; ++k)
+        if (!is_valid(cols[key_cols[k]].validity, r)) key_null = 1;
+    return (key_null && n_keys > 1) ? -1 : key_null;
+}
+
 int orc_groupby(uint64_t n, const orc_col* cols, int32_t n_cols,
                 const int32_t* key_cols, int32_t n_keys,
                 const orc_pred* preds, int32_t n_preds,
@@ -232,162 +433,223 @@ int orc_groupby(uint64_t n, const orc_col* cols, int32_t n_cols,
                 uint64_t cap, uint64_t* n_groups, char* err, int32_t err_cap) {
     (void)n_cols;
     if (n_keys < 1 || n_keys > 2 || n_aggs < 1) return ORC_INVALID;
-    for (int32_t a = 0; a < n_aggs; ++a) {
-        int op = aggs[a].op;
-        if (op == ORC_COUNT_STAR) continue;
-        const orc_col* c = &cols[aggs[a].input_col];
-        if ((op == ORC_SUM || op == ORC_AVG) && c->dtype == ORC_F32) return ORC_DECLINE;
-        if ((op == ORC_MIN || op == ORC_MAX || op == ORC_AVG) && c->dtype == ORC_DEC128)
-            return ORC_DECLINE;
-    }
-    omap m;
-    if (omap_init(&m, 1024)) return ORC_CAPACITY;
-    uint64_t ng = 0, gcap = 1024;
-    grp_t* groups = (grp_t*)malloc(gcap * sizeof(grp_t));
-    acc_t* acc = (acc_t*)calloc(gcap * (uint64_t)n_aggs, sizeof(acc_t));
-    int64_t null_group = -1;
-    int status = ORC_OK;
-
-    for (uint64_t r = 0; r < n; ++r) {
+    int st0 = gb_check_aggs(cols, aggs, n_aggs);
+    if (st0 != ORC_OK) return st0;
+    gb_state st;
+    if (gbs_init(&st, cols, key_cols, n_keys, aggs, n_aggs, 1024)) { gbs_free(&st); return ORC_CAPACITY; }
+    for (uint64_t r = 0; r < n && st.status != ORC_CAPACITY; ++r) {
         if (!orc_row_passes(cols, preds, n_preds, r)) continue;
-        int key_null = 0;
-        for (int32_t k = 0; k < n_keys; ++k)
-            if (!is_valid(cols[key_cols[k]].validity, r)) key_null = 1;
-        /* Multi-column keys drop NULL-key rows (groupby.rs:600-615); a
-         * single key column sends them to the one NULL group. */
-        if (key_null && n_keys > 1) continue;
-        uint32_t g;
-        if (key_null) {
-            if (null_group < 0) {
-                null_group = (int64_t)ng;
-                goto new_group;
+        const int key_null = gb_key_null(cols, key_cols, n_keys, r);
+        if (key_null < 0) continue;
+        gbs_fold_row(&st, r, key_null);
+    }
+    int status = st.status;
+    if (status == ORC_OVERFLOW) snprintf(err, err_cap, "%s", st.err);
+    if (status == ORC_OK && st.ng > cap) { *n_groups = st.ng; status = ORC_CAPACITY; }
+    if (status == ORC_OK) {
+        uint32_t* order = gbs_order(&st);
+        gbs_emit(&st, order, 0, out_keys, out_key_null, out_vals, out_valid, out_accurate);
+        free(order);
+        *n_groups = st.ng;
+    }
+    gbs_free(&st);
+    return status;
+}
+
+/* ---- GROUP BY on every host thread --------------------------------------- */
+/* The same fold run on T threads, with results identical to orc_groupby:
+ * rows are range-partitioned by their packed key (splitters from a sample of
+ * the keys), each partition is folded by one thread in row order (so every
+ * group sees its rows in the order the sequential fold does), sorted, and
+ * the partitions' outputs are concatenated in key order. The NULL group has
+ * a partition of its own, emitted last. */
+typedef struct {
+    uint64_t n;
+    const orc_col* cols;
+    const int32_t* key_cols;
+    int32_t n_keys;
+    const orc_pred* preds;
+    int32_t n_preds;
+    const orc_agg* aggs;
+    int32_t n_aggs;
+    int T;        /* threads */
+    int P;        /* key-range partitions (the NULL partition is P) */
+    const int64_t* splitters;  /* P - 1 ascending */
+    uint16_t* part;            /* per row: partition or 0xFFFF */
+    uint64_t* count;           /* [T][P + 1] */
+    uint64_t* off;             /* [T][P + 1] */
+    uint64_t* pbeg;            /* [P + 2] */
+    uint32_t* rows;            /* rows grouped by partition, row order inside */
+    gb_state* st;              /* [P + 1] */
+    uint32_t** order;          /* [P + 1] */
+    uint64_t* gbeg;            /* [P + 2] */
+    int64_t* out_keys;
+    uint8_t* out_key_null;
+    void** out_vals;
+    uint8_t** out_valid;
+    double** out_accurate;
+    int phase;
+    int next;                  /* dynamic partition counter */
+} gb_par;
+
+typedef struct { gb_par* g; int t; } gb_par_arg;
+
+static int upper_bound_i64(const int64_t* a, int n, int64_t k) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] <= k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+static void* gb_par_worker(void* vp) {
+    gb_par_arg* arg = (gb_par_arg*)vp;
+    gb_par* g = arg->g;
+    const int t = arg->t, P1 = g->P + 1;
+    const uint64_t r0 = g->n * (uint64_t)t / (uint64_t)g->T, r1 = g->n * (uint64_t)(t + 1) / (uint64_t)g->T;
+    if (g->phase == 0) {          /* classify rows of this thread's range */
+        uint64_t* cnt = g->count + (uint64_t)t * P1;
+        for (uint64_t r = r0; r < r1; ++r) {
+            uint16_t p = 0xFFFF;
+            if (orc_row_passes(g->cols, g->preds, g->n_preds, r)) {
+                const int kn = gb_key_null(g->cols, g->key_cols, g->n_keys, r);
+                if (kn == 1) p = (uint16_t)g->P;
+                else if (kn == 0)
+                    p = (uint16_t)upper_bound_i64(g->splitters, g->P - 1,
+                                                  orc_pack_key(g->cols, g->key_cols, g->n_keys, r));
             }
-            g = (uint32_t)null_group;
-        } else {
-            int ins;
-            int64_t key = orc_pack_key(cols, key_cols, n_keys, r);
-            if (ng * 2 >= m.cap && omap_grow(&m)) { status = ORC_CAPACITY; break; }
-            g = omap_get(&m, (uint64_t)key, (uint32_t)ng, &ins);
-            if (ins) goto new_group;
+            g->part[r] = p;
+            if (p != 0xFFFF) cnt[p]++;
         }
-        goto have_group;
-    new_group:
-        if (ng == gcap) {
-            uint64_t nc = gcap * 2;
-            groups = (grp_t*)realloc(groups, nc * sizeof(grp_t));
-            acc = (acc_t*)realloc(acc, nc * (uint64_t)n_aggs * sizeof(acc_t));
-            memset(acc + gcap * (uint64_t)n_aggs, 0, (nc - gcap) * (uint64_t)n_aggs * sizeof(acc_t));
-            gcap = nc;
+    } else if (g->phase == 1) {   /* scatter row numbers by partition */
+        uint64_t* off = g->off + (uint64_t)t * P1;
+        for (uint64_t r = r0; r < r1; ++r) {
+            const uint16_t p = g->part[r];
+            if (p != 0xFFFF) g->rows[off[p]++] = (uint32_t)r;
         }
-        g = (uint32_t)ng++;
-        groups[g].is_null = key_null;
-        groups[g].key = key_null ? INT64_MAX : orc_pack_key(cols, key_cols, n_keys, r);
-        groups[g].row_first = (uint32_t)r;
-    have_group:
-        for (int32_t a = 0; a < n_aggs; ++a) {
-            acc_t* s = &acc[(uint64_t)g * n_aggs + a];
-            int op = aggs[a].op;
-            if (op == ORC_COUNT_STAR) { s->cnt++; continue; }
-            const orc_col* c = &cols[aggs[a].input_col];
-            if (!is_valid(c->validity, r)) continue;
-            if (op == ORC_COUNT) { s->cnt++; continue; }
-            if (op == ORC_MIN || op == ORC_MAX) {
-                uint64_t k = mm_key(c, r);
-                if (s->cnt == 0) { s->mnk = s->mxk = k; }
-                else { if (k < s->mnk) s->mnk = k; if (k > s->mxk) s->mxk = k; }
-                s->cnt++;
+    } else if (g->phase == 2) {   /* fold and order whole partitions */
+        for (;;) {
+            const int p = __atomic_fetch_add(&g->next, 1, __ATOMIC_RELAXED);
+            if (p >= P1) break;
+            gb_state* s = &g->st[p];
+            const uint64_t b = g->pbeg[p], e = g->pbeg[p + 1];
+            if (gbs_init(s, g->cols, g->key_cols, g->n_keys, g->aggs, g->n_aggs, (e - b) / 64 + 1024)) {
+                s->status = ORC_CAPACITY;
                 continue;
             }
-            /* SUM / AVG */
-            s->cnt++;
-            if (is_float(c->dtype)) {
-                double v = col_f64(c, r);
-                s->fsum += v;
-                double t = s->csum + v;
-                if (fabs(s->csum) >= fabs(v)) s->comp += (s->csum - t) + v;
-                else s->comp += (v - t) + s->csum;
-                s->csum = t;
-            } else if (c->dtype == ORC_DEC128) {
-                i128 v = col_i128(c, r), out;
-                if (__builtin_add_overflow(s->isum, v, &out)) {
-                    if (status == ORC_OK) {
-                        snprintf(err, err_cap, "SUM(Decimal128) precision overflow: accumulator exceeds i128 range");
-                        status = ORC_OVERFLOW;
-                    }
-                } else s->isum = out;
-            } else {
-                int64_t v = col_i64(c, r);
-                if (c->dtype == ORC_I64 && op == ORC_SUM) {
-                    /* checked_group_sum (groupby.rs:1775): checked i64 add in row order */
-                    int64_t cur = (int64_t)s->isum, out;
-                    if (__builtin_add_overflow(cur, v, &out)) {
-                        if (status == ORC_OK) {
-                            snprintf(err, err_cap, "SUM(integer) overflow: accumulator exceeds i64 range");
-                            status = ORC_OVERFLOW;
-                        }
-                    } else s->isum = out;
-                } else {
-                    s->isum += v;
-                }
-            }
+            for (uint64_t i = b; i < e && s->status != ORC_CAPACITY; ++i) gbs_fold_row(s, g->rows[i], p == g->P);
+            g->order[p] = gbs_order(s);
+        }
+    } else {                      /* emit whole partitions at their offsets */
+        for (;;) {
+            const int p = __atomic_fetch_add(&g->next, 1, __ATOMIC_RELAXED);
+            if (p >= P1) break;
+            gbs_emit(&g->st[p], g->order[p], g->gbeg[p], g->out_keys, g->out_key_null, g->out_vals,
+                     g->out_valid, g->out_accurate);
         }
     }
-    if (status != ORC_OK) goto done;
-    if (ng > cap) { *n_groups = ng; status = ORC_CAPACITY; goto done; }
+    return NULL;
+}
 
-    /* Output order: packed key ascending as i64; NULL group last. */
+static void gb_par_run(gb_par* g, int phase) {
+    pthread_t th[256];
+    gb_par_arg args[256];
+    g->phase = phase;
+    g->next = 0;
+    for (int t = 0; t < g->T; ++t) {
+        args[t].g = g;
+        args[t].t = t;
+        if (t > 0) pthread_create(&th[t], NULL, gb_par_worker, &args[t]);
+    }
+    gb_par_worker(&args[0]);
+    for (int t = 1; t < g->T; ++t) pthread_join(th[t], NULL);
+}
+
+static int cmp_i64(const void* x, const void* y) {
+    const int64_t a = *(const int64_t*)x, b = *(const int64_t*)y;
+    return (a > b) - (a < b);
+}
+
+int orc_groupby_par(uint64_t n, const orc_col* cols, int32_t n_cols,
+                    const int32_t* key_cols, int32_t n_keys,
+                    const orc_pred* preds, int32_t n_preds,
+                    const orc_agg* aggs, int32_t n_aggs,
+                    int64_t* out_keys, uint8_t* out_key_null,
+                    void** out_vals, uint8_t** out_valid, double** out_accurate,
+                    uint64_t cap, uint64_t* n_groups, char* err, int32_t err_cap, int32_t threads) {
+    if (threads > 256) threads = 256;
+    if (threads <= 1 || n < 4096 || n >= 0xFFFFFFFFull)
+        return orc_groupby(n, cols, n_cols, key_cols, n_keys, preds, n_preds, aggs, n_aggs, out_keys,
+                           out_key_null, out_vals, out_valid, out_accurate, cap, n_groups, err, err_cap);
+    if (n_keys < 1 || n_keys > 2 || n_aggs < 1) return ORC_INVALID;
+    int st0 = gb_check_aggs(cols, aggs, n_aggs);
+    if (st0 != ORC_OK) return st0;
+    gb_par g;
+    memset(&g, 0, sizeof g);
+    g.n = n; g.cols = cols; g.key_cols = key_cols; g.n_keys = n_keys; g.preds = preds; g.n_preds = n_preds;
+    g.aggs = aggs; g.n_aggs = n_aggs; g.T = threads; g.P = threads * 8;
+    g.out_keys = out_keys; g.out_key_null = out_key_null; g.out_vals = out_vals; g.out_valid = out_valid;
+    g.out_accurate = out_accurate;
+    const int P1 = g.P + 1;
+    /* Splitters: row quantiles of a strided sample of the non-NULL keys. */
+    const uint64_t stride = n / 65536 + 1;
+    int64_t* sample = (int64_t*)malloc((n / stride + 1) * sizeof(int64_t));
+    uint64_t ns = 0;
+    for (uint64_t r = 0; r < n; r += stride)
+        if (orc_row_passes(cols, preds, n_preds, r) && gb_key_null(cols, key_cols, n_keys, r) == 0)
+            sample[ns++] = orc_pack_key(cols, key_cols, n_keys, r);
+    qsort(sample, ns, sizeof(int64_t), cmp_i64);
+    int64_t* spl = (int64_t*)malloc((size_t)g.P * sizeof(int64_t));
+    for (int i = 0; i + 1 < g.P; ++i) spl[i] = ns ? sample[(uint64_t)(i + 1) * ns / (uint64_t)g.P] : 0;
+    free(sample);
+    g.splitters = spl;
+    g.part = (uint16_t*)malloc(n * sizeof(uint16_t));
+    g.count = (uint64_t*)calloc((size_t)g.T * P1, sizeof(uint64_t));
+    g.off = (uint64_t*)calloc((size_t)g.T * P1, sizeof(uint64_t));
+    g.pbeg = (uint64_t*)calloc((size_t)P1 + 1, sizeof(uint64_t));
+    g.gbeg = (uint64_t*)calloc((size_t)P1 + 1, sizeof(uint64_t));
+    g.st = (gb_state*)calloc((size_t)P1, sizeof(gb_state));
+    g.order = (uint32_t**)calloc((size_t)P1, sizeof(uint32_t*));
+    int status = ORC_OK;
+    if (!g.part || !g.count || !g.off || !g.pbeg || !g.gbeg || !g.st || !g.order) { status = ORC_CAPACITY; goto out; }
+    gb_par_run(&g, 0);
     {
-        uint32_t* order = (uint32_t*)malloc((ng ? ng : 1) * sizeof(uint32_t));
-        grp_t* sorted = (grp_t*)malloc((ng ? ng : 1) * sizeof(grp_t));
-        for (uint64_t g = 0; g < ng; ++g) { sorted[g] = groups[g]; sorted[g].row_first = (uint32_t)g; }
-        qsort(sorted, ng, sizeof(grp_t), cmp_grp);
-        for (uint64_t g = 0; g < ng; ++g) order[g] = sorted[g].row_first;
-        for (uint64_t o = 0; o < ng; ++o) {
-            uint32_t g = order[o];
-            out_keys[o] = groups[g].is_null ? 0 : groups[g].key;
-            out_key_null[o] = (uint8_t)groups[g].is_null;
-            for (int32_t a = 0; a < n_aggs; ++a) {
-                const acc_t* s = &acc[(uint64_t)g * n_aggs + a];
-                int op = aggs[a].op;
-                uint8_t valid = 1;
-                const orc_col* c = op == ORC_COUNT_STAR ? NULL : &cols[aggs[a].input_col];
-                if (op == ORC_COUNT_STAR || op == ORC_COUNT) {
-                    ((int64_t*)out_vals[a])[o] = s->cnt;
-                } else if (op == ORC_MIN || op == ORC_MAX) {
-                    valid = s->cnt > 0;
-                    uint64_t k = op == ORC_MIN ? s->mnk : s->mxk;
-                    if (is_float(c->dtype)) ((double*)out_vals[a])[o] = valid ? mm_key_to_f64(k) : 0.0;
-                    else ((int64_t*)out_vals[a])[o] = valid ? (int64_t)(k ^ 0x8000000000000000ull) : 0;
-                } else if (op == ORC_SUM) {
-                    valid = s->cnt > 0;
-                    if (is_float(c->dtype)) {
-                        ((double*)out_vals[a])[o] = valid ? s->fsum : 0.0;
-                        if (out_accurate && out_accurate[a]) out_accurate[a][o] = s->csum + s->comp;
-                    } else if (c->dtype == ORC_DEC128) {
-                        i128 v = valid ? s->isum : 0;
-                        ((uint64_t*)out_vals[a])[2 * o] = (uint64_t)v;
-                        ((uint64_t*)out_vals[a])[2 * o + 1] = (uint64_t)((unsigned __int128)v >> 64);
-                    } else {
-                        ((int64_t*)out_vals[a])[o] = valid ? (int64_t)s->isum : 0;
-                    }
-                } else { /* AVG = (sum f64) / count (groupby.rs:2877-2885) */
-                    valid = s->cnt > 0;
-                    double sum = is_float(c->dtype) ? s->fsum : (double)s->isum;
-                    ((double*)out_vals[a])[o] = valid ? sum / (double)s->cnt : 0.0;
-                    if (out_accurate && out_accurate[a])
-                        out_accurate[a][o] = valid ? (is_float(c->dtype) ? (s->csum + s->comp) : (double)s->isum) / (double)s->cnt : 0.0;
-                }
-                if (out_valid && out_valid[a]) out_valid[a][o] = valid;
+        uint64_t tot = 0;
+        for (int p = 0; p < P1; ++p) {
+            g.pbeg[p] = tot;
+            for (int t = 0; t < g.T; ++t) {
+                g.off[(uint64_t)t * P1 + p] = tot;
+                tot += g.count[(uint64_t)t * P1 + p];
             }
         }
-        free(order);
-        free(sorted);
+        g.pbeg[P1] = tot;
+        g.rows = (uint32_t*)malloc((tot ? tot : 1) * sizeof(uint32_t));
+        if (!g.rows) { status = ORC_CAPACITY; goto out; }
     }
-    *n_groups = ng;
-done:
-    omap_free(&m);
-    free(groups);
-    free(acc);
+    gb_par_run(&g, 1);
+    gb_par_run(&g, 2);
+    /* The first failing partition in key order names the error. */
+    for (int p = 0; p < P1 && status == ORC_OK; ++p) {
+        status = g.st[p].status;
+        if (status == ORC_OVERFLOW) snprintf(err, err_cap, "%s", g.st[p].err);
+    }
+    if (status == ORC_OK) {
+        uint64_t ng = 0;
+        for (int p = 0; p < P1; ++p) { g.gbeg[p] = ng; ng += g.st[p].ng; }
+        *n_groups = ng;
+        if (ng > cap) status = ORC_CAPACITY;
+        else gb_par_run(&g, 3);
+    }
+out:
+    if (g.st)
+        for (int p = 0; p < P1; ++p) {
+            if (g.st[p].groups || g.st[p].acc || g.st[p].m.keys) gbs_free(&g.st[p]);
+            if (g.order) free(g.order[p]);
+        }
+    free(spl); free(g.part); free(g.count); free(g.off); free(g.pbeg); free(g.gbeg); free(g.st);
+    free(g.order); free(g.rows);
     return status;
 }
 

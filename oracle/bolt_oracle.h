@@ -53,6 +53,16 @@ int orc_groupby(uint64_t n, const orc_col* cols, int32_t n_cols,
                 void** out_vals, uint8_t** out_valid, double** out_accurate,
                 uint64_t cap, uint64_t* n_groups, char* err, int32_t err_cap);
 
+/* orc_groupby on `threads` host threads (range partitions of the packed key,
+ * each folded in row order by one thread): identical outputs and status. */
+int orc_groupby_par(uint64_t n, const orc_col* cols, int32_t n_cols,
+                    const int32_t* key_cols, int32_t n_keys,
+                    const orc_pred* preds, int32_t n_preds,
+                    const orc_agg* aggs, int32_t n_aggs,
+                    int64_t* out_keys, uint8_t* out_key_null,
+                    void** out_vals, uint8_t** out_valid, double** out_accurate,
+                    uint64_t cap, uint64_t* n_groups, char* err, int32_t err_cap, int32_t threads);
+
 /* Packs one row's key exactly as pack_keys (groupby_common.rs:352). */
 int64_t orc_pack_key(const orc_col* cols, const int32_t* key_cols, int32_t n_keys, uint64_t row);
 

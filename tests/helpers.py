@@ -72,33 +72,42 @@ def split_packed(packed: np.ndarray, dtypes: list[str]) -> list[np.ndarray]:
 
 
 def assert_float_close(got: np.ndarray, want: np.ndarray, rel: float = REL_TOL, what: str = "",
-                       accurate: np.ndarray | None = None):
+                       accurate: np.ndarray | None = None, stats: dict | None = None) -> int:
     """|got - want| <= rel * max(|got|, |want|, 1) against the sequential FP64
     oracle `want`. Where that fails, the value passes only if the oracle itself
     is the inaccurate one: `got` within rel of the compensated sum `accurate`
-    while `want` is not (a group whose sum nearly cancels can make a
-    sequential fold's own rounding error exceed 1e-12 * max(|S|, 1))."""
+    while `want` is not (a group whose sum nearly cancels, or a group of
+    millions of rows, can make a sequential fold's own rounding error exceed
+    1e-12 * max(|S|, 1)). Returns how many values passed only that way (also
+    added to stats[what] when `stats` is given)."""
     got = np.asarray(got, dtype=np.float64)
     want = np.asarray(want, dtype=np.float64)
     both_nan = np.isnan(got) & np.isnan(want)
     denom = np.maximum(np.maximum(np.abs(got), np.abs(want)), 1.0)
     with np.errstate(invalid="ignore"):
         bad = ~both_nan & ~(np.abs(got - want) <= rel * denom)
+    escaped = 0
     if bad.any() and accurate is not None:
         acc = np.asarray(accurate, dtype=np.float64)
         d_acc = np.maximum(np.maximum(np.abs(got), np.abs(acc)), 1.0)
         with np.errstate(invalid="ignore"):
             got_ok = np.abs(got - acc) <= rel * d_acc
             oracle_off = ~(np.abs(want - acc) <= rel * d_acc)
+        escaped = int((bad & got_ok & oracle_off).sum())
         bad = bad & ~(got_ok & oracle_off)
     if bad.any():
         i = int(np.flatnonzero(bad)[0])
         raise AssertionError(f"{what}: {int(bad.sum())} values differ, first at {i}: got {got[i]!r} want {want[i]!r}")
+    if stats is not None:
+        stats[what] = stats.get(what, 0) + escaped
+    return escaped
 
 
-def compare_groupby(res, orc: dict, group_by_dtypes: list[str], aggs: list, in_dtypes: list, rel: float = REL_TOL):
+def compare_groupby(res, orc: dict, group_by_dtypes: list[str], aggs: list, in_dtypes: list, rel: float = REL_TOL,
+                    stats: dict | None = None):
     """Compares a GroupbyResult with the oracle's output (bit-exact except
-    float SUM/AVG within `rel`)."""
+    float SUM/AVG within `rel`; `stats` collects, per float aggregate, how many
+    values passed through assert_float_close's compensated-sum check)."""
     g = orc["n_groups"]
     assert res.n_groups == g, f"group count {res.n_groups} != oracle {g}"
     want_keys = split_packed(orc["keys"], group_by_dtypes)
@@ -123,7 +132,7 @@ def compare_groupby(res, orc: dict, group_by_dtypes: list[str], aggs: list, in_d
             assert np.array_equal(got[m], want[m]), f"aggregate {a} (SUM dec128) differs"
         elif op in ("avg",) or (op == "sum" and in_dt in ("f32", "f64")):
             acc = orc["accurate"][a][m] if in_dt in ("f32", "f64") else None
-            assert_float_close(got[m], want[m], rel, f"aggregate {a} ({op})", accurate=acc)
+            assert_float_close(got[m], want[m], rel, f"aggregate {a} ({op})", accurate=acc, stats=stats)
         elif in_dt in ("f32", "f64"):
             gw = got[m].astype(np.float64)
             ww = want[m].astype(np.float64)

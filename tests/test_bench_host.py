@@ -65,7 +65,7 @@ def test_reduce_max_without_process_group_is_identity():
 def _reference_arm(rank: int) -> subprocess.CompletedProcess:
     env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", CUDA_VISIBLE_DEVICES="")
     cmd = [sys.executable, "bench.py", "--impl", "reference", "--steps", "3", "--warmup", "3",
-           "--reference-rows", "20000"]
+           "--rows", "20000"]
     return subprocess.run(cmd, cwd=REPO, env=env, capture_output=True, text=True, timeout=600)
 
 
@@ -77,6 +77,8 @@ def test_reference_arm_rank0_prints_one_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "rows/s"
     assert d["cpu_baseline"]["cores"] >= 1 and d["e2e"]["h2d_bytes_per_step"] == 0
+    # the reference arm times the whole configured workload every step
+    assert d["config"]["rows_per_step"] == 20000 and d["config"]["rows"] == 20000
 
 
 def test_reference_arm_other_ranks_exit_quietly():

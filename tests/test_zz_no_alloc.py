@@ -100,3 +100,25 @@ def test_noalloc_refuses_more_groups_than_its_table_holds(bolt, engine):
     st, msg = run_noalloc(bolt, pq)
     assert st == ERR_CAPACITY
     assert "6144 groups" in msg
+
+
+def test_noalloc_grows_past_a_low_hint(bolt, engine):
+    """A hint far below the real group count (10 vs about 3000) starts with a
+    small table; the call grows it within the array and returns what
+    bolt_groupby returns."""
+    table = make_table(bolt, 400_000, 3000, 34)
+    aggs = [("count_star", None), ("sum", "vi"), ("min", "vi"), ("max", "vd")]
+    want = engine.execute_groupby(table, ["k"], aggs, groups_hint=3000)
+    assert want.n_groups > 2500
+    pq = engine.prepare_groupby(table, ["k"], aggs, [], groups_hint=10, out_cap=8192)
+    st, msg = run_noalloc(bolt, pq)
+    assert st == 0, msg
+    assert_same(pq.result(False), want)
+
+
+def test_noalloc_output_capacity_below_the_group_count(bolt, engine):
+    table = make_table(bolt, 100_000, 2000, 35)
+    pq = engine.prepare_groupby(table, ["k"], [("count_star", None)], [], groups_hint=2000, out_cap=100)
+    st, msg = run_noalloc(bolt, pq)
+    assert st == ERR_CAPACITY
+    assert "capacity" in msg
