@@ -333,6 +333,12 @@ def gen_filtered(n: int, device: str | None):
     return dg.groupby_filtered(n, seed=2, cdf=cdf)
 
 
+def tier_flags(c: Ctx) -> int:
+    """GROUP BY flags for --tier: the library's choice, the shared-memory tier
+    over a global hash table, or the hash-partitioned tier."""
+    return {"auto": 0, "global": c.bolt.FLAG_NO_PART, "part": c.bolt.FLAG_FORCE_PART}[c.args.tier]
+
+
 class PreparedCall:
     """A prepared GROUP BY run through bolt_groupby with BOLT_FLAG_ASYNC."""
 
@@ -340,20 +346,28 @@ class PreparedCall:
         self.c, self.pq = c, pq
         self.ng = c.torch.zeros(1, dtype=c.torch.int64, device=c.dev)
         pq.out.n_groups_dev = self.ng.data_ptr()
+        self.flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE | tier_flags(c)
 
     def __call__(self):
         c = self.c
-        st = c.lib.bolt_groupby(c.eng._ctx, C.byref(self.pq.desc), C.byref(self.pq.out),
-                                c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE, C.c_void_p(c.stream.cuda_stream))
+        st = c.lib.bolt_groupby(c.eng._ctx, C.byref(self.pq.desc), C.byref(self.pq.out), self.flags,
+                                C.c_void_p(c.stream.cuda_stream))
         if st != 0:
             raise RuntimeError(f"bolt_groupby: {c.lib.bolt_ctx_last_error(c.eng._ctx).decode()}")
         return int(c.lib.bolt_ctx_last_launches(c.eng._ctx))
 
 
+PART_KERNELS = ("gb_spill_kernel + gb_part_count_kernel + gb_part_scan_kernel + gb_part_scatter_kernel + "
+                "gb_part_reduce_kernel (hash-partitioned tier)")
+
+
 def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
-    """Which aggregation kernel the timed GROUP BY runs: the staged kernel
-    when the tuning cache (or, untuned, the library's default for inputs
-    of 4M rows and more) chooses it, else the register-tile kernel."""
+    """Which aggregation kernels the timed GROUP BY runs: the partitioned
+    tier's five when --tier part or the tuning cache chooses it; else the
+    staged kernel when the tuning cache (or, untuned, the library's default
+    for inputs of 4M rows and more) chooses it, else the register-tile kernel."""
+    if c.args.tier == "part":
+        return PART_KERNELS
     staged = rows >= (1 << 22)
     if tuned:
         import tempfile
@@ -362,6 +376,8 @@ def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
             lines = [ln.split() for ln in open(f.name) if ln.strip() and not ln.startswith("#")]
         if len(lines) == 1 and len(lines[0]) >= 8:
             staged = int(lines[0][6]) > 0
+            if len(lines[0]) >= 9 and int(lines[0][8]) == 1 and c.args.tier == "auto":
+                return PART_KERNELS
     return "gb_staged_kernel" if staged else "gb_agg_kernel"
 
 
@@ -840,6 +856,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the GROUP BY autotuner")
     ap.add_argument("--tuning", default=None, help="load GROUP BY launch choices from this file instead of tuning")
     ap.add_argument("--save-tuning", default=None, help="write the GROUP BY launch choices to this file")
+    ap.add_argument("--tier", default="auto", choices=["auto", "global", "part"],
+                    help="GROUP BY tier: the library's choice, shared-memory + global hash table, hash-partitioned")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

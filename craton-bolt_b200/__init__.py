@@ -23,13 +23,13 @@ import numpy as np
 import torch
 
 from . import _abi
-from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLOBAL, FLAG_FORCE_SHMEM,
-                   FLAG_KERNEL_REGS, FLAG_KERNEL_STAGED, FLAG_NO_TUNE, FLAG_PROFILE)
+from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLOBAL, FLAG_FORCE_PART,
+                   FLAG_FORCE_SHMEM, FLAG_KERNEL_REGS, FLAG_KERNEL_STAGED, FLAG_NO_PART, FLAG_NO_TUNE, FLAG_PROFILE)
 
 __all__ = ["BoltError", "DeclineError", "SpillError", "TypeError_", "GpuCapacityError", "TimeoutError_",
            "CudaError", "PlanError", "Column", "Engine", "col", "GroupbyResult", "FLAG_ASYNC",
            "FLAG_PROFILE", "FLAG_FORCE_GLOBAL", "FLAG_FORCE_SHMEM", "FLAG_NO_TUNE", "FLAG_KERNEL_REGS",
-           "FLAG_KERNEL_STAGED", "lib", "PreparedGroupby",
+           "FLAG_KERNEL_STAGED", "FLAG_NO_PART", "FLAG_FORCE_PART", "lib", "PreparedGroupby",
            "Server", "BatchGraph"]
 
 
@@ -225,6 +225,12 @@ class Engine:
     @property
     def stream_handle(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
+
+    @property
+    def last_groupby_tier(self) -> int:
+        """Tier of the last GROUP BY: 1 shared-memory + global hash table,
+        2 hash-partitioned."""
+        return int(self._lib.bolt_ctx_last_groupby_tier(self._ctx))
 
     @property
     def scratch_bytes(self) -> int:

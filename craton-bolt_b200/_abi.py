@@ -37,6 +37,8 @@ FLAG_FORCE_SHMEM = 0x8
 FLAG_NO_TUNE = 0x10
 FLAG_KERNEL_REGS = 0x20
 FLAG_KERNEL_STAGED = 0x40
+FLAG_NO_PART = 0x80
+FLAG_FORCE_PART = 0x100
 
 
 class ColView(C.Structure):
@@ -88,6 +90,7 @@ SIGNATURES = {
     "bolt_status_str": (C.c_char_p, [C.c_int]),
     "bolt_ctx_last_device_ms": (C.c_double, [C.c_void_p]),
     "bolt_ctx_last_launches": (C.c_uint32, [C.c_void_p]),
+    "bolt_ctx_last_groupby_tier": (C.c_int32, [C.c_void_p]),
     "bolt_ctx_kernel_times": (C.c_uint32, [C.c_void_p, C.POINTER(C.c_double), C.c_uint32]),
     "bolt_ctx_sync_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bolt_ctx_scratch_bytes": (C.c_uint64, [C.c_void_p]),

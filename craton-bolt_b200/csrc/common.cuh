@@ -22,6 +22,7 @@ enum : uint32_t {
     ST_FLAG_DECRANGE = 1u << 6,  // decimal value does not fit the 64-bit fast path
     ST_FLAG_CAPACITY = 1u << 7,  // output capacity exceeded
     ST_FLAG_DECOVERFLOW = 1u << 8,  // SUM(Decimal128) outside the i128 range
+    ST_FLAG_INTERNAL = 1u << 9,     // a finalize index outside its table (never expected)
 };
 
 // Bytes per row of a column dtype (0 for an unknown dtype).

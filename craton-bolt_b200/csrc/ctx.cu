@@ -120,6 +120,7 @@ bolt_status flags_to_status(bolt_ctx* ctx, uint32_t f, const char* op) {
     if (f & ST_FLAG_SPILL) return fail(ctx, BOLT_ERR_SPILL, "partition_reduce spill: %s hash table probe limit reached", op);
     if (f & ST_FLAG_DUPKEY) return fail(ctx, BOLT_DECLINE, "%s: duplicate build keys", op);
     if (f & ST_FLAG_CAPACITY) return fail(ctx, BOLT_ERR_CAPACITY, "%s: output capacity exceeded", op);
+    if (f & ST_FLAG_INTERNAL) return fail(ctx, BOLT_ERR_CUDA, "%s: internal error (group index outside its table)", op);
     return BOLT_OK;
 }
 
@@ -225,6 +226,7 @@ uint32_t bolt_ctx_kernel_times(bolt_ctx* ctx, double* ms, uint32_t max) {
 const char* bolt_ctx_last_error(const bolt_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 double bolt_ctx_last_device_ms(const bolt_ctx* ctx) { return ctx ? ctx->last_ms : 0.0; }
 uint32_t bolt_ctx_last_launches(const bolt_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
+int32_t bolt_ctx_last_groupby_tier(const bolt_ctx* ctx) { return ctx ? ctx->last_tier : 0; }
 uint64_t bolt_ctx_scratch_bytes(const bolt_ctx* ctx) { return ctx ? ctx->arena_bytes : 0; }
 
 bolt_status bolt_ctx_sync_status(bolt_ctx* ctx, bolt_stream stream) {

@@ -32,6 +32,7 @@ struct bolt_ctx {
     uint32_t kcount = 0;
     double last_ms = 0.0;
     uint32_t last_launches = 0;
+    int32_t last_tier = 0;       // GROUP BY tier of the last bolt_groupby (1 global table, 2 partitioned)
     uint32_t async_pending = 0;
     std::string last_error;
     // Pinned staging ring for descriptor uploads: each upload copies into the
@@ -48,9 +49,14 @@ struct bolt_ctx {
     // Autotuned GROUP BY launch choices per query shape (see gb_shape_key).
     // GROUP BY launch choices: block size, shared-table shrink (8 = no shared
     // tier), warp pre-aggregation, table load (1 << load_shift - 1 headroom),
-    // shared-table admission in eighths, and the staged kernel's 32-row
-    // chunks per consumer warp (0 = the register kernel).
-    struct GbTune { int32_t block, smem_shift, warp_agg, load_shift, smem_fill, staged; double ms; };
+    // shared-table admission in eighths, the staged kernel's 32-row chunks
+    // per consumer warp (0 = the register kernel), and whether the
+    // hash-partitioned tier serves the shape (part = 1).
+    struct GbTune {
+        int32_t block, smem_shift, warp_agg, load_shift, smem_fill, staged;
+        double ms;
+        int32_t part = 0;
+    };
     std::unordered_map<uint64_t, GbTune> tune;
     // Host-column GROUP BY (bolt_groupby_host): a copy stream and, per
     // staging slot, "copied" / "consumed" events; created on first use.

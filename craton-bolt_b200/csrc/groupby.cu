@@ -29,6 +29,7 @@
 // call and it is re-run with plain f64 atomics (the reference's own method).
 #include "groupby.cuh"
 #include "gb_device.cuh"
+#include "groupby_part.cuh"
 #include "join.cuh"
 #include "radix_sort.cuh"
 #include "bulk.cuh"
@@ -651,7 +652,7 @@ __global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fin
         __syncthreads();
         load_final(f, fins + q);
         const ull cap = 1ull << f.log2cap;
-        const ull G = *f.n_nonnull;
+        const ull G = min(*f.n_nonnull, f.n_max);  // (a counter that ran past the table flagged GROW)
         const bool has_null = f.gtab[(cap + 1) * (ull)f.slot_words] != 0;
         const ull total = G + (has_null ? 1 : 0);
         const uint64_t c0 = (uint64_t)(item - begins[q]) * FIN_CHUNK;
@@ -662,7 +663,14 @@ __global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fin
         }
         const ull lim = total < f.out_cap ? total : f.out_cap;
         const uint64_t c1 = c0 + FIN_CHUNK < lim ? c0 + FIN_CHUNK : lim;
-        for (uint64_t o = c0 + threadIdx.x; o < c1; o += blockDim.x) emit_group(f, o, o < G ? f.sorted[o] : cap + 1);
+        for (uint64_t o = c0 + threadIdx.x; o < c1; o += blockDim.x) {
+            const uint64_t slot = o < G ? f.sorted[o] : cap + 1;
+            if (slot > cap + 1) {  // (a sort entry nobody wrote: never read past the table)
+                atomicOr(f.status, ST_FLAG_INTERNAL);
+                continue;
+            }
+            emit_group(f, o, slot);
+        }
     }
 }
 
@@ -1162,6 +1170,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     // 10K-row query hinted at 1M groups would otherwise clear and scan an
     // 8M-slot table.
     const uint64_t hint = d->groups_hint ? std::min<uint64_t>(d->groups_hint, n + 2) : 0;
+    pl->groups_hint = hint;
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
     pl->shape = gb_shape_key(p, n, hint);
     // Untuned default: the register kernel for small inputs, the staged
@@ -1192,6 +1201,7 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     else cap = 1ull << ceil_log2_u64(std::max<uint64_t>(std::min<uint64_t>(2 * n + 16, 1ull << 16), 64));
     pl->cap = cap;
     p.log2cap = f.log2cap = ceil_log2_u64(cap);
+    f.n_max = cap + 1;
     p.max_probe = (uint32_t)std::min<uint64_t>(cap, 1u << 14);
     p.grow_limit = cap - cap / 4;
     p.row_begin = row_begin;
@@ -1483,9 +1493,11 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
             GbPlan* pl = pls[large_q[i]];
             GbFinal& f = pl->fin;
             const uint64_t g = pl->cap + 1;
-            f.order_keys = (ull*)arena_alloc(ctx, g * 8);
-            f.slots = (uint32_t*)arena_alloc(ctx, g * 4);
-            f.sorted = (uint32_t*)arena_alloc(ctx, g * 4);
+            if (!pl->precompacted) {  // (the partitioned tier wrote the sort keys itself)
+                f.order_keys = (ull*)arena_alloc(ctx, g * 8);
+                f.slots = (uint32_t*)arena_alloc(ctx, g * 4);
+                f.sorted = (uint32_t*)arena_alloc(ctx, g * 4);
+            }
             if (!f.order_keys || !f.slots || !f.sorted)
                 return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
             large.push_back(f);
@@ -1496,7 +1508,7 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
             seg.payload_in = f.slots;
             seg.payload_out = f.sorted;
             seg.n_dev = f.n_nonnull;
-            seg.n = g;
+            seg.n = f.n_max;
             sp.segs.push_back(seg);
         }
         cbeg[nl] = (uint32_t)citems;
@@ -1507,8 +1519,10 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
         if (st == BOLT_OK) st = stage_upload(ctx, s, d_beg, cbeg.data(), 4ull * (nl + 1));
         if (st != BOLT_OK) return st;
         const unsigned cg = (unsigned)std::min<uint64_t>(citems, (uint64_t)ctx->num_sms * 8);
-        gb_compact_batch_kernel<<<cg, 256, 0, s>>>(d_f, d_beg, nl, (uint32_t)citems);
-        ctx->last_launches++;
+        if (!pls[large_q[0]]->precompacted) {  // (a precompacted query is finalized alone)
+            gb_compact_batch_kernel<<<cg, 256, 0, s>>>(d_f, d_beg, nl, (uint32_t)citems);
+            ctx->last_launches++;
+        }
         st = radix_sort(ctx, s, sp);
         if (st != BOLT_OK) return st;
         gb_gather_batch_kernel<<<cg, 256, 0, s>>>(d_f, d_beg, nl, (uint32_t)citems);
@@ -1545,6 +1559,46 @@ extern "C" uint64_t bolt_groupby_footprint(const bolt_groupby_desc* desc, uint64
 }
 
 namespace bolt {
+
+// Runs one query on the hash-partitioned tier: the compact group array
+// (cap + 2 slots; only the two special slots start at zero, pass C writes
+// every other slot it uses), the per-query words, the finalize buffers that
+// pass C fills with the groups' sort keys, the partitioned passes and the
+// finalize.
+static bolt_status gb_run_part(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags, int pbits) {
+    GbParams& p = pl->prm;
+    GbFinal& f = pl->fin;
+    const uint64_t slot_bytes = (uint64_t)p.slot_words * 8;
+    const uint64_t table = ((pl->cap + 2) * slot_bytes + 255) & ~uint64_t(255);
+    char* region = (char*)arena_alloc(ctx, table + 256);
+    const uint64_t g = pl->cap + 1;
+    f.order_keys = (ull*)arena_alloc(ctx, g * 8);
+    f.slots = (uint32_t*)arena_alloc(ctx, g * 4);
+    f.sorted = (uint32_t*)arena_alloc(ctx, g * 4);
+    if (!region || !f.order_keys || !f.slots || !f.sorted)
+        return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the group array");
+    ull* w = (ull*)(region + table);
+    BOLT_CUDA(ctx, cudaMemsetAsync(region + pl->cap * slot_bytes, 0, 2 * slot_bytes, s));
+    BOLT_CUDA(ctx, cudaMemsetAsync(w, 0, 256, s));
+    p.gtab = (ull*)region;
+    p.occupancy = w;
+    p.status = ctx->d_status;
+    p.i64_bits = nullptr;
+    for (int s2 = 0; s2 < p.n_st; ++s2)
+        if (p.st[s2].kind == K_SUM_I64) p.i64_bits = (uint32_t*)(w + 4);
+    f.gtab = p.gtab;
+    f.n_nonnull = w + 1;
+    f.n_groups = w + 2;
+    f.status = p.status;
+    f.n_max = pl->cap;
+    pl->words = w;
+    pl->precompacted = true;
+    pl->small_final = false;
+    bolt_status st = gb_part_launch(ctx, pl, s, flags, pbits);
+    if (st != BOLT_OK) return st;
+    GbPlan* one = pl;
+    return gb_run_finalize(ctx, &one, 1, s);
+}
 
 // The reference checks SUM(Int64) with a checked add in row order per group
 // (checked_group_sum, groupby.rs:1775-1798), so a prefix that leaves the
@@ -1585,12 +1639,69 @@ static bolt_status gb_single(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_gro
                              const bolt_col_view* jkey, const char* op) {
     int mode = 0;
     uint64_t cap_override = 0;
-    for (int attempt = 0; attempt < 6; ++attempt) {
+    int part_pbits = 0;       // partitions (log2) after a partition spilled
+    bool no_part = false;     // the partitioned tier gave way to the global table
+    uint64_t groups_seen = 0; // groups an earlier attempt counted (sizes the next one)
+    for (int attempt = 0; attempt < 8; ++attempt) {
         bolt_status st = call_begin(ctx, flags, s);
         if (st != BOLT_OK) return st;
         GbPlan pl;
         st = gb_plan(ctx, d, out, rb, re, flags, mode, cap_override, &pl);
         if (st != BOLT_OK) return st;
+        pl.groups_hint = std::max<uint64_t>(pl.groups_hint, groups_seen);
+        if (!jt && !no_part && gb_part_applies(ctx, pl, flags)) {
+            ctx->last_tier = 2;
+            pl.fin.n_groups_user = (flags & BOLT_FLAG_ASYNC) ? (ull*)out->n_groups_dev : nullptr;
+            st = gb_run_part(ctx, &pl, s, flags, part_pbits);
+            if (st == BOLT_DECLINE || st == BOLT_ERR_CAPACITY) {
+                // No kernel for this layout, or no room for the spill
+                // segments: the global-table path serves the query.
+                ctx->last_error.clear();
+                no_part = true;
+                continue;
+            }
+            if (st != BOLT_OK) return st;
+            st = call_end(ctx, flags, s);
+            if (st != BOLT_OK) return st;
+            if (flags & BOLT_FLAG_ASYNC) return BOLT_OK;
+            uint32_t f = 0;
+            st = read_status(ctx, s, 0, &f);
+            if (st != BOLT_OK) return st;
+            ull w[5] = {0, 0, 0, 0, 0};
+            BOLT_CUDA(ctx, cudaMemcpy(w, pl.words, sizeof w, cudaMemcpyDeviceToHost));
+            out->n_groups = w[2];
+            const uint32_t bits = (uint32_t)w[4];
+            if (f == 0 && pl.prm.i64_bits && bits + (uint32_t)ceil_log2_u64(pl.prm.n_rows + 1) >= 63) {
+                // The row-order SUM(Int64) check replays rows against a hash
+                // table of the groups: run the query on the global table.
+                no_part = true;
+                continue;
+            }
+            // The group counter (w[1]) counts past the array, so it sizes the
+            // retry; after a spill it is a lower bound.
+            if (f & ST_FLAG_SPILL) {
+                // A partition outgrew its table (or a segment its room):
+                // 4x the partitions, then the global table.
+                groups_seen = std::max<uint64_t>(groups_seen, 2 * w[1]);
+                if (pl.part_pbits + 2 <= GB_PART_MAX_PBITS) part_pbits = pl.part_pbits + 2;
+                else no_part = true;
+                continue;
+            }
+            if (f & ST_FLAG_GROW) {
+                groups_seen = std::max<uint64_t>(groups_seen, w[1]);
+                cap_override = std::max<uint64_t>(pl.cap * 2, 1ull << ceil_log2_u64(w[1] + w[1] / 4 + 16));
+                continue;
+            }
+            if (f & (ST_FLAG_RANGE | ST_FLAG_DECRANGE)) {
+                if (f & ST_FLAG_RANGE) mode |= GB_MODE_F64_ATOMIC;
+                if (f & ST_FLAG_DECRANGE) mode |= GB_MODE_WIDE_DEC;
+                continue;
+            }
+            if (f & ST_FLAG_DECOVERFLOW)
+                return fail(ctx, BOLT_ERR_OVERFLOW, "SUM(Decimal128) precision overflow: accumulator exceeds i128 range");
+            return flags_to_status(ctx, f, op);
+        }
+        ctx->last_tier = 1;
         if (jt) {
             pl.prm.jslots = jt->slots;
             pl.prm.jlog2cap = jt->log2cap;
@@ -2140,6 +2251,12 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             for (int warp_agg : {0, 1})
                 for (int load_shift : {0, 1, 2})
                     for (int smem_fill : {2, 3, 4, 6}) cands.push_back({512, smem_shift, warp_agg, load_shift, smem_fill, staged, 0.0});
+    // The hash-partitioned tier, with two admission caps of its shared table.
+    for (int smem_fill : {3, 4}) {
+        bolt_ctx::GbTune c{512, 0, 0, 1, smem_fill, 2, 0.0};
+        c.part = 1;
+        cands.push_back(c);
+    }
     bolt_ctx::GbTune best{512, 1, 0, 1, 4, 0, 1e30};
     const bool verbose = std::getenv("BOLT_TUNE_VERBOSE") != nullptr;
     uint64_t shape = 0;
@@ -2153,13 +2270,19 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
             st = gb_plan(ctx, desc, out, 0, nrows, 0, 0, 0, &pl, &c);
             if (st != BOLT_OK) return st;
             shape = pl.shape;
-            if (c.staged && !gb_staged_layout(ctx, pl, nullptr)) {
-                ok = false;  // the staged kernel does not apply to this query
+            if (c.part ? !gb_part_applies(ctx, pl, BOLT_FLAG_FORCE_PART)
+                       : (c.staged && !gb_staged_layout(ctx, pl, nullptr))) {
+                ok = false;  // the candidate's kernels do not apply to this query
                 break;
             }
             BOLT_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
             GbPlan* one = &pl;
-            st = gb_run(ctx, &one, 1, s, 0);
+            st = c.part ? gb_run_part(ctx, &pl, s, 0, 0) : gb_run(ctx, &one, 1, s, 0);
+            if (st == BOLT_DECLINE || st == BOLT_ERR_CAPACITY) {
+                ctx->last_error.clear();
+                ok = false;
+                break;
+            }
             if (st != BOLT_OK) return st;
             BOLT_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
             uint32_t f = 0;
@@ -2175,9 +2298,9 @@ extern "C" bolt_status bolt_groupby_autotune(bolt_ctx* ctx, const bolt_groupby_d
         }
         if (verbose)
             std::fprintf(stderr,
-                         "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem_fill=%d/8 staged=%d -> "
-                         "%s%.4f ms\n",
-                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem_fill, c.staged,
+                         "[bolt autotune] block=%d smem_shift=%d warp_agg=%d load_shift=%d smem_fill=%d/8 staged=%d "
+                         "part=%d -> %s%.4f ms\n",
+                         c.block, c.smem_shift, c.warp_agg, c.load_shift, c.smem_fill, c.staged, c.part,
                          ok ? "" : "(not eligible) ", tot / 2);
         if (ok && tot / 2 < best.ms) {
             best = c;
@@ -2195,9 +2318,9 @@ extern "C" bolt_status bolt_ctx_tuning_save(const bolt_ctx* ctx, const char* pat
     FILE* fp = std::fopen(path, "w");
     if (!fp) return BOLT_ERR_INVALID;
     for (const auto& kv : ctx->tune)
-        std::fprintf(fp, "%llx %d %d %d %d %d %d %.6f\n", (unsigned long long)kv.first, kv.second.block,
+        std::fprintf(fp, "%llx %d %d %d %d %d %d %.6f %d\n", (unsigned long long)kv.first, kv.second.block,
                      kv.second.smem_shift, kv.second.warp_agg, kv.second.load_shift, kv.second.smem_fill,
-                     kv.second.staged, kv.second.ms);
+                     kv.second.staged, kv.second.ms, kv.second.part);
     std::fclose(fp);
     return BOLT_OK;
 }
@@ -2207,10 +2330,15 @@ extern "C" bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path) {
     FILE* fp = std::fopen(path, "r");
     if (!fp) return fail(ctx, BOLT_ERR_INVALID, "tuning file %s not readable", path);
     unsigned long long key;
-    bolt_ctx::GbTune t{};
-    while (std::fscanf(fp, "%llx %d %d %d %d %d %d %lf", &key, &t.block, &t.smem_shift, &t.warp_agg, &t.load_shift,
-                       &t.smem_fill, &t.staged, &t.ms) == 8) {
-        const bool valid = (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
+    char line[256];
+    // One shape per line; the tier column (part) is optional (older files).
+    while (std::fgets(line, sizeof line, fp)) {
+        bolt_ctx::GbTune t{};
+        const int got = std::sscanf(line, "%llx %d %d %d %d %d %d %lf %d", &key, &t.block, &t.smem_shift, &t.warp_agg,
+                                    &t.load_shift, &t.smem_fill, &t.staged, &t.ms, &t.part);
+        if (got < 8) continue;
+        if (got == 8) t.part = 0;
+        const bool valid = (t.part == 0 || t.part == 1) && (t.block == 256 || t.block == 512) && t.smem_shift >= 0 &&
                            t.smem_shift <= 8 && (t.warp_agg == 0 || t.warp_agg == 1) && t.load_shift >= 0 &&
                            t.load_shift <= 3 && t.smem_fill >= 1 && t.smem_fill <= 8 &&
                            (t.staged == 0 || t.staged == 1 || t.staged == 2 || t.staged == 4);

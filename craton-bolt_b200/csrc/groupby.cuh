@@ -138,6 +138,11 @@ struct alignas(16) GbFinal {
     ull* n_groups;       // device: groups written (incl. NULL group)
     ull* n_groups_user;  // optional user device word
     uint32_t* status;
+    // Most sort entries (order_keys / slots) the aggregation can have
+    // written: cap + 1 for the global table, cap for the partitioned tier's
+    // compact array (its group counter may run past it when the array must
+    // grow; entries beyond were never written).
+    ull n_max;
 };
 
 // A fully planned GROUP BY (one query).
@@ -162,7 +167,7 @@ struct GbPlan {
     // per tile, the partition count used (log2), and whether the finalize
     // finds the groups already compacted with their sort keys.
     int32_t part_hot_log2 = 0;
-    int32_t part_chunks = 1;
+    int32_t part_chunks = 2;
     int32_t part_pbits = 0;
     bool precompacted = false;
 };

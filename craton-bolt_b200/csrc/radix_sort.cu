@@ -136,7 +136,13 @@ __device__ __forceinline__ int seg_of(const uint32_t* begins, int nseg, uint32_t
     return lo;
 }
 
-__device__ __forceinline__ uint64_t seg_n(const SegDesc& d) { return d.n_dev ? *d.n_dev : d.n; }
+// Rows of a segment: the device count when given, never more than the
+// segment's buffers hold (a producer that ran out of room may count past it).
+__device__ __forceinline__ uint64_t seg_n(const SegDesc& d) {
+    if (!d.n_dev) return d.n;
+    const uint64_t n = *d.n_dev;
+    return n < d.n ? n : d.n;
+}
 
 template <typename K>
 __global__ void __launch_bounds__(256) sort_hist_kernel(SortArgs a) {

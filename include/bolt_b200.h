@@ -113,6 +113,10 @@ const char* bolt_status_str(bolt_status s);
 double      bolt_ctx_last_device_ms(const bolt_ctx* ctx);
 /* Number of kernels the last call launched (all are this library's). */
 uint32_t    bolt_ctx_last_launches(const bolt_ctx* ctx);
+/* Which GROUP BY tier served the last bolt_groupby on this context: 1 = the
+ * shared-memory tier over a global hash table, 2 = the hash-partitioned tier
+ * (the reference's Tier-1 / Tier-2 executors); 0 before any GROUP BY. */
+int32_t     bolt_ctx_last_groupby_tier(const bolt_ctx* ctx);
 /* Device milliseconds of the dominant kernel of every call made with
  * BOLT_FLAG_PROFILE since the previous read (up to 256 calls, oldest first).
  * Waits for those kernels; returns how many times were written to `ms`. */

@@ -137,26 +137,37 @@ def test_join_groupby_full_size_against_torch_join(bolt, big_engine):
     assert bool((sums.data[:, 1] == 0).all())
 
 
-def test_groupby_filtered_full_size_vs_oracle(bolt, big_engine, oracle):
-    """Config 2 at its own size, per group against the oracle. The escape
-    count is how many f64 SUM / AVG values matched the compensated sum but
-    not the sequential fold (whose own rounding error grows with a group's
-    row count: the Zipf head group holds ~5.8M filtered rows)."""
+@pytest.fixture(scope="module")
+def filtered_full(oracle):
+    """Config 2's 100M rows (host numpy) and the oracle's result on them."""
     b = bench_mod()
-    n = 100_000_000
-    data = b.gen_filtered(n, "cuda:0")
-    dev = {k: bolt.Column(torch.from_numpy(v).cuda(), b.FILTERED_DT[k]) for k, v in data.items()}
-    res = big_engine.execute_groupby(dev, ["a", "b"], b.FILTERED_AGGS, where=[("f", "<", 50)],
-                                     groups_hint=4_000_000)
-    del dev
+    data = b.gen_filtered(100_000_000, "cuda:0")
     host = {k: oracle.HostCol(v, b.FILTERED_DT[k]) for k, v in data.items()}
     t0 = time.perf_counter()
     orc = oracle.groupby(host, ["a", "b"], b.FILTERED_AGGS, where=[("f", "<", 50)], threads=oracle.host_threads())
-    t_orc = time.perf_counter() - t0
+    return data, orc, time.perf_counter() - t0
+
+
+@pytest.mark.parametrize("tier", ["global", "part"])
+def test_groupby_filtered_full_size_vs_oracle(bolt, big_engine, oracle, filtered_full, tier):
+    """Config 2 at its own size, per group against the oracle, on each tier
+    (the shared-memory + global hash table tier and the hash-partitioned
+    tier). The escape count is how many f64 SUM / AVG values matched the
+    compensated sum but not the sequential fold (whose own rounding error
+    grows with a group's row count: the Zipf head group holds ~5.8M
+    filtered rows)."""
+    b = bench_mod()
+    data, orc, t_orc = filtered_full
+    dev = {k: bolt.Column(torch.from_numpy(v).cuda(), b.FILTERED_DT[k]) for k, v in data.items()}
+    flags = bolt.FLAG_NO_PART if tier == "global" else bolt.FLAG_FORCE_PART
+    res = big_engine.execute_groupby(dev, ["a", "b"], b.FILTERED_AGGS, where=[("f", "<", 50)],
+                                     groups_hint=4_000_000, flags=flags)
+    assert big_engine.last_groupby_tier == (1 if tier == "global" else 2)
+    del dev
     stats = {}
     compare_groupby(res, orc, ["i32", "i32"], b.FILTERED_AGGS, ["f64", "f64", None, "i64", "i64"], REL_TOL, stats)
-    print(f"\n[full-size GROUP BY] {orc['n_groups']} groups, oracle {t_orc:.1f} s on {oracle.host_threads()} "
-          f"threads; values matched via the compensated sum only: {stats}")
+    print(f"\n[full-size GROUP BY, {tier} tier] {orc['n_groups']} groups, oracle {t_orc:.1f} s on "
+          f"{oracle.host_threads()} threads; values matched via the compensated sum only: {stats}")
     assert orc["n_groups"] > 3_000_000
     # the compensated-sum path is for the large groups whose sequential sum drifts
     assert sum(stats.values()) <= orc["n_groups"] // 1000
