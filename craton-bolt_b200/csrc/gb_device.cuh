@@ -373,6 +373,57 @@ __device__ __forceinline__ void gb_flush_absbits(const GbParams& p, uint32_t& ab
     absbits = 0;
 }
 
+// Per-warp occupancy accounting after a tile (whole warp, no block barrier):
+// new keys are added to the query's counter in batches, and the warp learns
+// whether the query already flagged growth or a spill (then it stops).
+__device__ __forceinline__ bool gb_warp_epilogue(const GbParams& p, uint32_t& inserts, uint32_t& pending) {
+    pending += __reduce_add_sync(0xffffffffu, inserts);
+    inserts = 0;
+    const uint32_t batch = p.log2cap > 20 ? 256u : (p.log2cap > 12 ? (1u << (p.log2cap - 12)) : 1u);
+    uint32_t stop = 0;
+    if (lane_id() == 0) {
+        if (pending >= batch) {
+            const ull tot = atomicAdd(p.occupancy, (ull)pending) + pending;
+            if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
+        }
+        stop = (*reinterpret_cast<volatile uint32_t*>(p.status) & (ST_FLAG_GROW | ST_FLAG_SPILL)) != 0;
+    }
+    if (pending >= batch) pending = 0;
+    return __shfl_sync(0xffffffffu, stop, 0) != 0;
+}
+
+// Adds a warp's not yet published key count to the query's counter.
+__device__ __forceinline__ void gb_warp_flush_pending(const GbParams& p, uint32_t& pending) {
+    if (lane_id() == 0 && pending) {
+        const ull tot = atomicAdd(p.occupancy, (ull)pending) + pending;
+        if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
+    }
+    pending = 0;
+}
+
+// Merges a CTA's shared table into the query's global table (whole CTA,
+// after a __syncthreads()).
+__device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk, const ull* sw, int C) {
+    const int SW = p.sslot_words - 1;
+    uint32_t inserts = 0;
+    for (int i = threadIdx.x; i < C; i += blockDim.x) {
+        const ull key = sk[i];
+        if (key == 0) continue;
+        const int64_t g = g_find_insert(p, key, inserts);
+        if (g < 0) continue;
+        ull* w = p.gtab + (ull)g * p.slot_words;
+        const ull* src = sw + (ull)i * SW - 1;
+        for (int s = 0; s < p.n_st; ++s) {
+            const StateDesc& d = p.st[s];
+            merge_partial(w + d.word, d.kind, src + d.sword);
+        }
+    }
+    if (inserts) {
+        const ull tot = atomicAdd(p.occupancy, (ull)inserts) + inserts;
+        if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Reads from a staged tile (shared memory) or straight from the columns
 // ---------------------------------------------------------------------------

@@ -217,57 +217,6 @@ __device__ __forceinline__ void gb_process_tile(const GbParams& p, ull* sk, ull*
     }
 }
 
-// Per-warp occupancy accounting after a tile (whole warp, no block barrier):
-// new keys are added to the query's counter in batches, and the warp learns
-// whether the query already flagged growth or a spill (then it stops).
-__device__ __forceinline__ bool gb_warp_epilogue(const GbParams& p, uint32_t& inserts, uint32_t& pending) {
-    pending += __reduce_add_sync(0xffffffffu, inserts);
-    inserts = 0;
-    const uint32_t batch = p.log2cap > 20 ? 256u : (p.log2cap > 12 ? (1u << (p.log2cap - 12)) : 1u);
-    uint32_t stop = 0;
-    if (lane_id() == 0) {
-        if (pending >= batch) {
-            const ull tot = atomicAdd(p.occupancy, (ull)pending) + pending;
-            if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
-        }
-        stop = (*reinterpret_cast<volatile uint32_t*>(p.status) & (ST_FLAG_GROW | ST_FLAG_SPILL)) != 0;
-    }
-    if (pending >= batch) pending = 0;
-    return __shfl_sync(0xffffffffu, stop, 0) != 0;
-}
-
-// Adds a warp's not yet published key count to the query's counter.
-__device__ __forceinline__ void gb_warp_flush_pending(const GbParams& p, uint32_t& pending) {
-    if (lane_id() == 0 && pending) {
-        const ull tot = atomicAdd(p.occupancy, (ull)pending) + pending;
-        if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
-    }
-    pending = 0;
-}
-
-// Merges a CTA's shared table into the query's global table (whole CTA,
-// after a __syncthreads()).
-__device__ __forceinline__ void gb_flush_shared(const GbParams& p, const ull* sk, const ull* sw, int C) {
-    const int SW = p.sslot_words - 1;
-    uint32_t inserts = 0;
-    for (int i = threadIdx.x; i < C; i += blockDim.x) {
-        const ull key = sk[i];
-        if (key == 0) continue;
-        const int64_t g = g_find_insert(p, key, inserts);
-        if (g < 0) continue;
-        ull* w = p.gtab + (ull)g * p.slot_words;
-        const ull* src = sw + (ull)i * SW - 1;
-        for (int s = 0; s < p.n_st; ++s) {
-            const StateDesc& d = p.st[s];
-            merge_partial(w + d.word, d.kind, src + d.sword);
-        }
-    }
-    if (inserts) {
-        const ull tot = atomicAdd(p.occupancy, (ull)inserts) + inserts;
-        if (tot > p.grow_limit) atomicOr(p.status, ST_FLAG_GROW);
-    }
-}
-
 template <int U, int MAXS, class SP>
 __global__ void __launch_bounds__(512, SP::generic ? 1 : 2) gb_agg_kernel(const __grid_constant__ GbParams p) {
     extern __shared__ __align__(16) ull smem[];
@@ -1344,6 +1293,12 @@ static bolt_status gb_run_tables(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStream
 
 // Launches the aggregation of one query (the single-query kernels).
 static bolt_status gb_agg_one(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags) {
+    // Dense shapes of 4M+ rows: the streaming kernel compiled for the key,
+    // WHERE and state layouts (groupby_part.cu), misses to the global table.
+    if (!(flags & BOLT_FLAG_KERNEL_STAGED) && pl->tune.staged != 0) {
+        bolt_status st = BOLT_OK;
+        if (gb_lean_global(ctx, pl, s, flags, &st)) return st;
+    }
     GbParams& p = pl->prm;
     size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.sslot_words;
     const uint64_t tile = (uint64_t)pl->block * pl->u;

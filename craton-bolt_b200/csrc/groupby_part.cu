@@ -146,70 +146,140 @@ __device__ __forceinline__ void row_contrib(const GbParams& p, const GbPart& q, 
     }
 }
 
-// One warp step of up to 32 surviving rows of a tile (row i valid when has):
-// fold into the CTA's shared table or append to the CTA's spill segment.
-template <int KP, class SP>
-__device__ __forceinline__ void spill_step(const GbParams& p, const GbPart& q, ull* sk, ull* sw, uint32_t* fill,
-                                           uint32_t* s_nspill, uint32_t* s_stop, bool has, uint32_t i,
-                                           const TileCols& t, uint32_t& absbits) {
-    constexpr int NF = GB_PART_MAX_FIELDS;
+// What the streaming kernel does with a surviving row whose key is not in
+// the CTA's shared table.
+constexpr int MISS_SPILL = 0;   // append it to the CTA's spill segment (partitioned tier)
+constexpr int MISS_GLOBAL = 1;  // fold it into the global hash table (global-table tier)
+
+// Absent-key filter: one bit per hash of every key admitted to the CTA's
+// shared table. Once the table admits no more keys, a row whose bit is clear
+// is a miss without a probe (most misses under skew). A bit set after a
+// concurrent lookup read it clear only sends that row down the miss path,
+// which is correct for every row.
+constexpr int FILT_WORDS = 2048;  // 65,536 bits, 8 KB
+
+// Per-warp state of the streaming consumer.
+struct LeanWarp {
+    uint32_t absbits;  // largest |v| bit length fed to an Int64 SUM
+    uint32_t inserts;  // new global-table keys (MISS_GLOBAL), not yet counted
+    uint32_t pending;  // ... counted per warp, not yet published
+    // Survivors carried to the next tile so that every fold step has 32
+    // rows: lanes below npend hold a row (key + value words, loaded).
+    uint32_t npend;
+    ull pstored;
+    ull pfw[GB_PART_MAX_FIELDS];
+};
+
+// Key and value words of row i.
+template <int KP>
+__device__ __forceinline__ void load_row(const GbPart& q, const TileCols& t, uint32_t i, ull& stored,
+                                         ull (&fw)[GB_PART_MAX_FIELDS]) {
+    stored = stored_key<KP>(t, i);
+#pragma unroll
+    for (int f = 0; f < GB_PART_MAX_FIELDS; ++f) fw[f] = f < q.n_fields ? field_val(q, t, f, i) : 0ull;
+}
+
+// Shared-table find-or-insert from a precomputed home slot; an admitted key
+// sets its filter bit. -1 when the key is absent and the table admits no
+// more keys (or the probe window ends).
+__device__ __forceinline__ int hot_find_insert(ull* sk, uint32_t mask, uint32_t h, ull stored, uint32_t* fill,
+                                               uint32_t limit, uint32_t* filt, uint32_t fb) {
+    volatile ull* vk = sk;
+    for (int i = 0; i < SMEM_PROBES; ++i) {
+        const ull k = vk[h];
+        if (k == stored) return (int)h;
+        if (k == 0) {
+            if (*reinterpret_cast<volatile uint32_t*>(fill) >= limit) return -1;
+            const ull old = atomicCAS(&sk[h], 0ull, stored);
+            if (old == 0) {
+                atomicAdd(fill, 1u);
+                atomicOr(&filt[fb >> 5], 1u << (fb & 31));
+                return (int)h;
+            }
+            if (old == stored) return (int)h;
+        }
+        h = (h + 1) & mask;
+    }
+    return -1;
+}
+
+// One warp step: up to 32 rows (lane's row valid when has) folded into the
+// CTA's shared table, the misses handled per MISS.
+template <class SP, int MISS>
+__device__ __forceinline__ void fold_step(const GbParams& p, const GbPart& q, ull* sk, ull* sw, uint32_t* fill,
+                                          uint32_t* filt, uint32_t* s_nspill, uint32_t* s_stop, bool has, ull stored,
+                                          const ull (&fw)[GB_PART_MAX_FIELDS], LeanWarp& lw) {
     const uint32_t lane = lane_id();
     const int SW = p.sslot_words - 1;
-    ull stored = 0;
-    ull fw[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) fw[f] = 0;
-    if (has) {
-        stored = stored_key<KP>(t, i);
-#pragma unroll
-        for (int f = 0; f < NF; ++f)
-            if (f < q.n_fields) fw[f] = field_val(q, t, f, i);
-    }
-    // The key whose complement is 0 keeps its own slot of the group array.
+    // The key whose complement is 0 keeps its own slot of the group table.
     if (has && stored == 0) {
         ull c0[SP::n], c1[SP::n];
-        row_contrib<SP>(p, q, fw, c0, c1, absbits);
+        row_contrib<SP>(p, q, fw, c0, c1, lw.absbits);
         ull* w = p.gtab + (1ull << p.log2cap) * (ull)p.slot_words;
         if (ld_volatile(w) == 0) *reinterpret_cast<volatile ull*>(w) = 1ull;
 #pragma unroll
         for (int s = 0; s < SP::n; ++s) merge_words(w + p.st[s].word, SP::kind(s), c0[s], c1[s]);
         has = false;
     }
-    const int sl = has ? s_find_insert(sk, p.smem_log2, stored, fill, p.smem_fill) : -1;
+    int sl = -1;
+    if (has) {
+        const ull hp = stored * HASH_S;
+        const uint32_t fb = (uint32_t)hp >> 16;
+        const bool maybe = (filt[fb >> 5] >> (fb & 31)) & 1u;
+        if (maybe || *reinterpret_cast<volatile uint32_t*>(fill) < p.smem_fill)
+            sl = hot_find_insert(sk, (1u << p.smem_log2) - 1, (uint32_t)(hp >> (64 - p.smem_log2)), stored, fill,
+                                 p.smem_fill, filt, fb);
+    }
     if (sl >= 0) {
         ull c0[SP::n], c1[SP::n];
-        row_contrib<SP>(p, q, fw, c0, c1, absbits);
+        row_contrib<SP>(p, q, fw, c0, c1, lw.absbits);
         ull* w = sw + (ull)sl * SW - 1;
 #pragma unroll
         for (int s = 0; s < SP::n; ++s) merge_words_smem(w + p.st[s].sword, SP::kind(s), c0[s], c1[s], true);
     }
     const bool miss = has && sl < 0;
-    const uint32_t mm = __ballot_sync(0xffffffffu, miss);
-    if (mm == 0) return;
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(s_nspill, (uint32_t)__popc(mm));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (!miss) return;
-    const uint64_t pos = (uint64_t)base + __popc(mm & lanemask_lt());
-    if (pos >= q.seg_stride) {  // the segment is full: the host re-plans
-        atomicOr(p.status, ST_FLAG_SPILL);
-        *reinterpret_cast<volatile uint32_t*>(s_stop) = 1u;
-        return;
-    }
-    const uint64_t at = (uint64_t)blockIdx.x * q.seg_stride + pos;
-    q.skey[at] = stored;
+    if constexpr (MISS == MISS_GLOBAL) {
+        if (miss) {
+            const int64_t g = g_find_insert(p, stored, lw.inserts);
+            if (g >= 0) {
+                ull c0[SP::n], c1[SP::n];
+                row_contrib<SP>(p, q, fw, c0, c1, lw.absbits);
+                ull* w = p.gtab + (ull)g * p.slot_words;
 #pragma unroll
-    for (int f = 0; f < NF; ++f)
-        if (f < q.n_fields) q.sfield[f][at] = fw[f];
+                for (int s = 0; s < SP::n; ++s) merge_words(w + p.st[s].word, SP::kind(s), c0[s], c1[s]);
+            }
+        }
+    } else {
+        const uint32_t mm = __ballot_sync(0xffffffffu, miss);
+        if (mm == 0) return;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(s_nspill, (uint32_t)__popc(mm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (!miss) return;
+        const uint64_t pos = (uint64_t)base + __popc(mm & lanemask_lt());
+        if (pos >= q.seg_stride) {  // the segment is full: the host re-plans
+            atomicOr(p.status, ST_FLAG_SPILL);
+            *reinterpret_cast<volatile uint32_t*>(s_stop) = 1u;
+            return;
+        }
+        const uint64_t at = (uint64_t)blockIdx.x * q.seg_stride + pos;
+        q.skey[at] = stored;
+#pragma unroll
+        for (int f = 0; f < GB_PART_MAX_FIELDS; ++f)
+            if (f < q.n_fields) q.sfield[f][at] = fw[f];
+    }
 }
 
 // Filters the rows [first, first + 32 * nchunks) of a tile (tile-relative,
 // below `limit`) into the warp's list with a range test on the WHERE column,
-// then folds / spills the survivors 32 to a warp step.
-template <int KP, class SP>
-__device__ __forceinline__ void spill_rows(const GbParams& p, const GbPart& q, ull* sk, ull* sw, uint32_t* fill,
-                                           uint32_t* s_nspill, uint32_t* s_stop, const TileCols& t, uint32_t first,
-                                           int nchunks, uint32_t limit, uint16_t* list, uint32_t& absbits) {
+// then folds the survivors in steps of 32: the rows carried from earlier
+// tiles fill the first step, and the survivors that would leave the last
+// step part-empty are carried on (loaded into registers, so the stage can
+// be released).
+template <int KP, class SP, int MISS>
+__device__ __forceinline__ void lean_rows(const GbParams& p, const GbPart& q, ull* sk, ull* sw, uint32_t* fill,
+                                          uint32_t* filt, uint32_t* s_nspill, uint32_t* s_stop, const TileCols& t,
+                                          uint32_t first, int nchunks, uint32_t limit, uint16_t* list, LeanWarp& lw) {
     const uint32_t lane = lane_id();
     uint32_t cnt = 0;
     const int32_t* pc = reinterpret_cast<const int32_t*>(t.pc);
@@ -225,23 +295,38 @@ __device__ __forceinline__ void spill_rows(const GbParams& p, const GbPart& q, u
         cnt += __popc(m);
     }
     __syncwarp();
-    for (uint32_t b = 0; b < cnt; b += 32) {
-        const bool has = b + lane < cnt;
-        const uint32_t i = first + (has ? (uint32_t)list[b + lane] : 0u);
-        spill_step<KP, SP>(p, q, sk, sw, fill, s_nspill, s_stop, has, i, t, absbits);
+    uint32_t b = 0;  // survivors of this tile already taken
+    while (lw.npend + (cnt - b) >= 32) {
+        ull stored, fw[GB_PART_MAX_FIELDS];
+        if (lane < lw.npend) {
+            stored = lw.pstored;
+#pragma unroll
+            for (int f = 0; f < GB_PART_MAX_FIELDS; ++f) fw[f] = lw.pfw[f];
+        } else {
+            load_row<KP>(q, t, first + list[b + lane - lw.npend], stored, fw);
+        }
+        fold_step<SP, MISS>(p, q, sk, sw, fill, filt, s_nspill, s_stop, true, stored, fw, lw);
+        b += 32 - lw.npend;
+        lw.npend = 0;
     }
+    const uint32_t left = cnt - b;
+    if (lane >= lw.npend && lane < lw.npend + left)
+        load_row<KP>(q, t, first + list[b + lane - lw.npend], lw.pstored, lw.pfw);
+    lw.npend += left;
     __syncwarp();
 }
 
-// Pass A. Warp 0's lane 0 streams tiles of every staged column into a ring
-// of stages (bulk copies completing on the stage's `full` mbarrier); the
-// other warps filter, fold and spill, and release stages on `empty`. All
-// waits are bounded. Shared memory: stages | table keys | table states |
-// per-warp survivor lists; the stages hold the partial records' partition
-// histogram after the ring has drained.
-template <int KP, class SP>
-__global__ void __launch_bounds__(1024, 1) gb_spill_kernel(const __grid_constant__ GbParams p,
-                                                           const __grid_constant__ GbPart q) {
+// The streaming kernel (pass A of the partitioned tier with MISS_SPILL; the
+// global-table tier's aggregation with MISS_GLOBAL). Warp 0's lane 0
+// streams tiles of every staged column into a ring of stages (bulk copies
+// completing on the stage's `full` mbarrier); the other warps filter, fold
+// and handle misses, and release stages on `empty`. All waits are bounded.
+// Shared memory: stages | table keys | table states | filter | per-warp
+// survivor lists; with MISS_SPILL the stages hold the partial records'
+// partition histogram after the ring has drained.
+template <int KP, class SP, int MISS>
+__global__ void __launch_bounds__(1024, 1) gb_lean_kernel(const __grid_constant__ GbParams p,
+                                                          const __grid_constant__ GbPart q) {
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ __align__(8) uint64_t full[PART_MAX_STAGES], empty[PART_MAX_STAGES];
     __shared__ uint32_t s_fill, s_nspill, s_npart, s_stop;
@@ -251,15 +336,16 @@ __global__ void __launch_bounds__(1024, 1) gb_spill_kernel(const __grid_constant
     const uint32_t lane = lane_id();
     const int SW = p.sslot_words - 1;
     const int C = 1 << p.smem_log2;
-    const uint32_t P = 1u << q.pbits;
     unsigned char* stages = dsm;
     ull* sk = reinterpret_cast<ull*>(dsm + (size_t)S * p.stage_bytes);
     ull* sw = sk + C;
-    uint16_t* lists = reinterpret_cast<uint16_t*>(sw + (size_t)C * SW);
+    uint32_t* filt = reinterpret_cast<uint32_t*>(sw + (size_t)C * SW);
+    uint16_t* lists = reinterpret_cast<uint16_t*>(filt + FILT_WORDS);
     const uint32_t T = p.tile_rows;
     const uint64_t ntiles = p.n_rows / T;
 
     for (int i = threadIdx.x; i < C * (SW + 1); i += blockDim.x) sk[i] = 0;
+    for (int i = threadIdx.x; i < FILT_WORDS; i += blockDim.x) filt[i] = 0;
     if (threadIdx.x == 0) {
         s_fill = 0;
         s_nspill = 0;
@@ -273,7 +359,7 @@ __global__ void __launch_bounds__(1024, 1) gb_spill_kernel(const __grid_constant
     }
     __syncthreads();
 
-    uint32_t absbits = 0;
+    LeanWarp lw{};
     if (warp == 0) {
         if (lane == 0) {
             const uint64_t pol = l2_evict_first_policy();
@@ -327,11 +413,16 @@ __global__ void __launch_bounds__(1024, 1) gb_spill_kernel(const __grid_constant
             const bool stop = *reinterpret_cast<volatile uint32_t*>(&s_stop) != 0;
             if (!stop) {
                 const TileCols tc = tile_cols(p, q, stages + (size_t)st * p.stage_bytes, true, t * T);
-                spill_rows<KP, SP>(p, q, sk, sw, &s_fill, &s_nspill, &s_stop, tc,
-                                   (uint32_t)cw * 32u * (uint32_t)p.chunks, p.chunks, T, list, absbits);
+                lean_rows<KP, SP, MISS>(p, q, sk, sw, &s_fill, filt, &s_nspill, &s_stop, tc,
+                                        (uint32_t)cw * 32u * (uint32_t)p.chunks, p.chunks, T, list, lw);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);
+            if constexpr (MISS == MISS_GLOBAL) {
+                // Occupancy of the global table; growth or a spill stops the CTA.
+                if (gb_warp_epilogue(p, lw.inserts, lw.pending) && lane == 0)
+                    *reinterpret_cast<volatile uint32_t*>(&s_stop) = 1u;
+            }
         }
         // Rows after the last whole tile, 32 per consumer warp, from global memory.
         const uint64_t rem0 = ntiles * T;
@@ -339,32 +430,45 @@ __global__ void __launch_bounds__(1024, 1) gb_spill_kernel(const __grid_constant
         if (rem) {
             const TileCols tc = tile_cols(p, q, nullptr, false, rem0);
             for (uint32_t c = (uint32_t)(blockIdx.x * NW + cw) * 32u; c < rem; c += gridDim.x * (uint32_t)NW * 32u)
-                spill_rows<KP, SP>(p, q, sk, sw, &s_fill, &s_nspill, &s_stop, tc, c, 1, rem, list, absbits);
+                lean_rows<KP, SP, MISS>(p, q, sk, sw, &s_fill, filt, &s_nspill, &s_stop, tc, c, 1, rem, list, lw);
+        }
+        // The rows still carried.
+        if (lw.npend)
+            fold_step<SP, MISS>(p, q, sk, sw, &s_fill, filt, &s_nspill, &s_stop, lane < lw.npend, lw.pstored,
+                                lw.pfw, lw);
+        if constexpr (MISS == MISS_GLOBAL) {
+            lw.pending += __reduce_add_sync(0xffffffffu, lw.inserts);
+            gb_warp_flush_pending(p, lw.pending);
         }
     }
-    gb_flush_absbits(p, absbits);
+    gb_flush_absbits(p, lw.absbits);
     __syncthreads();
-    const uint32_t g = blockIdx.x;
-    if (threadIdx.x == 0) q.n_spill[g] = (uint64_t)s_nspill < q.seg_stride ? s_nspill : (uint32_t)q.seg_stride;
-    // The shared table as partial-state records (shared-table slot layout),
-    // counted per partition in the (drained) stage memory.
-    uint32_t* hist = reinterpret_cast<uint32_t*>(stages);
-    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) hist[i] = 0;
-    __syncthreads();
-    const int W = SW + 1;
-    for (int i = threadIdx.x; i < C; i += blockDim.x) {
-        const ull key = sk[i];
-        if (key == 0) continue;
-        const uint32_t pos = atomicAdd(&s_npart, 1u);  // pos < C
-        ull* dst = q.ppart + ((uint64_t)g * q.hot_cap + pos) * (uint64_t)W;
-        dst[0] = key;
-        const ull* src = sw + (ull)i * SW;
-        for (int k = 0; k < SW; ++k) dst[1 + k] = src[k];
-        atomicAdd(&hist[part_of(key, q.pbits)], 1u);
+    if constexpr (MISS == MISS_GLOBAL) {
+        gb_flush_shared(p, sk, sw, C);
+    } else {
+        const uint32_t P = 1u << q.pbits;
+        const uint32_t g = blockIdx.x;
+        if (threadIdx.x == 0) q.n_spill[g] = (uint64_t)s_nspill < q.seg_stride ? s_nspill : (uint32_t)q.seg_stride;
+        // The shared table as partial-state records (shared-table slot
+        // layout), counted per partition in the (drained) stage memory.
+        uint32_t* hist = reinterpret_cast<uint32_t*>(stages);
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const int W = SW + 1;
+        for (int i = threadIdx.x; i < C; i += blockDim.x) {
+            const ull key = sk[i];
+            if (key == 0) continue;
+            const uint32_t pos = atomicAdd(&s_npart, 1u);  // pos < C
+            ull* dst = q.ppart + ((uint64_t)g * q.hot_cap + pos) * (uint64_t)W;
+            dst[0] = key;
+            const ull* src = sw + (ull)i * SW;
+            for (int k = 0; k < SW; ++k) dst[1 + k] = src[k];
+            atomicAdd(&hist[part_of(key, q.pbits)], 1u);
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) q.cnt_par[(uint64_t)g * P + i] = hist[i];
+        if (threadIdx.x == 0) q.n_part[g] = s_npart;
     }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) q.cnt_par[(uint64_t)g * P + i] = hist[i];
-    if (threadIdx.x == 0) q.n_part[g] = s_npart;
 }
 
 // Pass B1. CTA g counts segment g's rows per partition.
@@ -662,27 +766,28 @@ __global__ void __launch_bounds__(512) gb_part_reduce_kernel(const __grid_consta
     gb_flush_absbits(p, absbits);
 }
 
-using SpillKernel = void (*)(GbParams, GbPart);
+using LeanKernel = void (*)(GbParams, GbPart);
 using ReduceKernel = void (*)(GbParams, GbPart, ull*, ull*, uint32_t*);
 
-template <int KP>
-SpillKernel spill_for_spec(int spec) {
+template <int KP, int MISS>
+LeanKernel lean_for_spec(int spec) {
     switch (spec) {
-    case 1: return gb_spill_kernel<KP, Spec1>;
-    case 2: return gb_spill_kernel<KP, Spec2>;
-    case 4: return gb_spill_kernel<KP, Spec4>;
-    case 5: return gb_spill_kernel<KP, Spec5>;
-    case 6: return gb_spill_kernel<KP, Spec6>;
-    case 7: return gb_spill_kernel<KP, Spec7>;
+    case 1: return gb_lean_kernel<KP, Spec1, MISS>;
+    case 2: return gb_lean_kernel<KP, Spec2, MISS>;
+    case 4: return gb_lean_kernel<KP, Spec4, MISS>;
+    case 5: return gb_lean_kernel<KP, Spec5, MISS>;
+    case 6: return gb_lean_kernel<KP, Spec6, MISS>;
+    case 7: return gb_lean_kernel<KP, Spec7, MISS>;
     default: return nullptr;
     }
 }
 
-SpillKernel spill_kernel_for(int kp, int spec) {
+template <int MISS>
+LeanKernel lean_kernel_for(int kp, int spec) {
     switch (kp) {
-    case GB_KP_I32X2: return spill_for_spec<GB_KP_I32X2>(spec);
-    case GB_KP_I32: return spill_for_spec<GB_KP_I32>(spec);
-    default: return spill_for_spec<GB_KP_I64>(spec);
+    case GB_KP_I32X2: return lean_for_spec<GB_KP_I32X2, MISS>(spec);
+    case GB_KP_I32: return lean_for_spec<GB_KP_I32, MISS>(spec);
+    default: return lean_for_spec<GB_KP_I64, MISS>(spec);
     }
 }
 
@@ -727,17 +832,13 @@ void pred_range(int cmp, ll lit, int32_t& lo, int32_t& hi, int32_t& neg) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-bool gb_part_applies(const bolt_ctx* ctx, const GbPlan& pl, uint32_t flags) {
+bool gb_lean_applies(const GbPlan& pl, uint32_t flags) {
     const GbParams& p = pl.prm;
-    if (flags & (BOLT_FLAG_FORCE_GLOBAL | BOLT_FLAG_FORCE_SHMEM | BOLT_FLAG_KERNEL_REGS | BOLT_FLAG_NO_PART))
-        return false;
+    if (flags & (BOLT_FLAG_FORCE_GLOBAL | BOLT_FLAG_FORCE_SHMEM | BOLT_FLAG_KERNEL_REGS)) return false;
     if (p.jslots || p.spec == 0 || p.spec == 3 || p.n_rows < (1ull << 22) || p.n_rows >= (1ull << 31)) return false;
-    // Used when forced, or when the autotuner found it the faster tier for
-    // this query shape (and the shape expects many groups).
-    const bool forced = (flags & BOLT_FLAG_FORCE_PART) != 0;
-    if (!forced && (!pl.tune.part || pl.groups_hint < GB_PART_MIN_GROUPS)) return false;
     // Dense columns only; 32-bit integer keys (one or two) or one 64-bit
-    // integer key; at most one WHERE conjunct, on a 32-bit integer column.
+    // integer key; at most one WHERE conjunct, on a 32-bit integer column;
+    // at most GB_PART_MAX_FIELDS distinct value columns.
     for (int k = 0; k < p.n_keys; ++k) {
         if (p.kvalid[k]) return false;
         const int dt = p.kdtype[k];
@@ -758,17 +859,36 @@ bool gb_part_applies(const bolt_ctx* ctx, const GbPlan& pl, uint32_t flags) {
         if (is_value) ++nf;
     }
     if (nf > GB_PART_MAX_FIELDS) return false;
-    (void)ctx;
+    for (int c = 0; c < p.n_sc; ++c)  // bulk copies need 16-byte aligned tile starts
+        if (((uintptr_t)p.sc_col[c] + p.row_begin * (uint64_t)p.sc_w[c]) % 16 != 0) return false;
     return true;
 }
 
-// Plans and launches passes A, B1, S, B2 and C for one query whose compact
-// group array, words and finalize buffers are set up (see the header).
-bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags, int pbits_override) {
+bool gb_part_applies(const bolt_ctx* ctx, const GbPlan& pl, uint32_t flags) {
+    (void)ctx;
+    if ((flags & BOLT_FLAG_NO_PART) || !gb_lean_applies(pl, flags)) return false;
+    // Used when forced, or when the autotuner found it the faster tier for
+    // this query shape (and the shape expects many groups).
+    const bool forced = (flags & BOLT_FLAG_FORCE_PART) != 0;
+    return forced || (pl.tune.part && pl.groups_hint >= GB_PART_MIN_GROUPS);
+}
+
+namespace {
+
+// Launch shape of the streaming kernel, shared by both miss policies.
+struct LeanShape {
+    LeanKernel kernel;
+    int block;
+    size_t smem;
+};
+
+// Fills the value-field, predicate and staging parts of q and p for the
+// streaming kernel: 1 producer + 31 consumer warps, tiles of 31 x 32 x
+// chunks rows, as many stages (2..PART_MAX_STAGES) as fit beside the shared
+// table, the absent-key filter and the survivor lists.
+template <int MISS>
+bolt_status lean_setup(bolt_ctx* ctx, GbPlan* pl, GbPart& q, LeanShape& out) {
     GbParams& p = pl->prm;
-    GbFinal& fin = pl->fin;
-    GbPart q{};
-    // Fields: the distinct value columns, in state order.
     q.n_fields = 0;
     int field_of_sc[GB_MAX_SC];
     for (int c = 0; c < GB_MAX_SC; ++c) field_of_sc[c] = -1;
@@ -780,7 +900,7 @@ bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t f
         if (c < 0) continue;
         if (field_of_sc[c] < 0) {
             if (q.n_fields == GB_PART_MAX_FIELDS)
-                return fail(ctx, BOLT_DECLINE, "GROUP BY: more value columns than the partitioned tier carries");
+                return fail(ctx, BOLT_DECLINE, "GROUP BY: more value columns than the streaming kernel carries");
             field_of_sc[c] = q.n_fields;
             q.field_sc[q.n_fields] = (int8_t)c;
             q.field_w[q.n_fields] = (int8_t)dtype_width(dt);
@@ -792,47 +912,30 @@ bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t f
     q.has_pred = p.n_pred == 1;
     if (q.has_pred) pred_range(p.pred[0].cmp, p.pred[0].lit_i, q.pred_lo, q.pred_hi, q.pred_neg);
     const int kp = p.n_keys == 2 ? GB_KP_I32X2 : (p.kdtype[0] == BOLT_I32 ? GB_KP_I32 : GB_KP_I64);
-    const SpillKernel kA = spill_kernel_for(kp, p.spec);
-    const ReduceKernel kC = reduce_kernel_for(p.spec);
-    if (!kA || !kC) return fail(ctx, BOLT_DECLINE, "GROUP BY: no partitioned-tier kernel for this layout");
+    out.kernel = lean_kernel_for<MISS>(kp, p.spec);
+    if (!out.kernel) return fail(ctx, BOLT_DECLINE, "GROUP BY: no streaming kernel for this layout");
 
-    // Pass A launch shape: 1 producer + 31 consumer warps, tiles of
-    // 31 x 32 x chunks rows, as many stages (2..PART_MAX_STAGES) as fit
-    // beside the shared table and the survivor lists.
     const int chunks = std::max(1, std::min(pl->part_chunks, 2));
     const int block = 1024, nw = block / 32 - 1;
     const uint32_t T = (uint32_t)(nw * 32 * chunks);
     uint64_t row_w = 0;
-    for (int c = 0; c < p.n_sc; ++c) {
-        if (((uintptr_t)p.sc_col[c] + p.row_begin * (uint64_t)p.sc_w[c]) % 16 != 0)
-            return fail(ctx, BOLT_DECLINE, "GROUP BY: partitioned tier needs 16-byte aligned columns");
-        row_w += (uint64_t)p.sc_w[c];
-    }
-    const uint64_t groups = std::max<uint64_t>(pl->groups_hint, 1024);
-    // Partitions: about RED_GROUPS expected groups each.
-    int pbits = pbits_override > 0 ? pbits_override
-                                   : ceil_log2_u64((groups + GB_PART_RED_GROUPS - 1) / GB_PART_RED_GROUPS);
-    pbits = std::max(6, std::min(pbits, GB_PART_MAX_PBITS));
-    q.pbits = pbits;
-    const uint32_t P = 1u << pbits;
+    for (int c = 0; c < p.n_sc; ++c) row_w += (uint64_t)p.sc_w[c];
     const size_t stage = (size_t)T * row_w;
     const size_t lists = (size_t)nw * 32 * chunks * 2;
+    const size_t filt = (size_t)FILT_WORDS * 4;
     const size_t budget = (size_t)std::max(ctx->max_smem_optin - 1024, 0);
     const size_t entry = 8ull * (size_t)p.sslot_words;
     int sl = pl->part_hot_log2 > 0 ? pl->part_hot_log2 : 11;
     int S = 0;
     for (;;) {
         const size_t table = ((size_t)1 << sl) * entry;
-        if (table + lists + 2 * stage <= budget) {
-            S = (int)std::min<size_t>(PART_MAX_STAGES, (budget - table - lists) / stage);
+        if (table + filt + lists + 2 * stage <= budget) {
+            S = (int)std::min<size_t>(PART_MAX_STAGES, (budget - table - filt - lists) / stage);
             break;
         }
-        if (sl <= 8) return fail(ctx, BOLT_DECLINE, "GROUP BY: partitioned tier does not fit shared memory");
+        if (sl <= 8) return fail(ctx, BOLT_DECLINE, "GROUP BY: streaming kernel does not fit shared memory");
         --sl;
     }
-    // The drained stages hold the partial-record histogram (P words).
-    if ((size_t)S * stage < (size_t)P * 4)
-        return fail(ctx, BOLT_DECLINE, "GROUP BY: partitioned tier stages smaller than the histogram");
     p.smem_log2 = sl;
     // Admission: a fraction of the table (eighths), so a key that is absent
     // meets an empty slot after a few probes.
@@ -846,10 +949,65 @@ bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t f
         p.sc_off[c] = off;
         off += T * (uint32_t)p.sc_w[c];
     }
-    const size_t smemA = (size_t)S * stage + ((size_t)1 << sl) * entry + lists;
-    const int G = ctx->num_sms;
-    q.grid_a = G;
+    q.grid_a = ctx->num_sms;
     q.hot_cap = 1 << sl;
+    out.block = block;
+    out.smem = (size_t)S * stage + ((size_t)1 << sl) * entry + filt + lists;
+    return BOLT_OK;
+}
+
+}  // namespace
+
+bool gb_lean_global(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags, bolt_status* st) {
+    if (!gb_lean_applies(*pl, flags)) return false;
+    GbPart q{};
+    LeanShape sh;
+    *st = lean_setup<MISS_GLOBAL>(ctx, pl, q, sh);
+    if (*st == BOLT_DECLINE) {
+        ctx->last_error.clear();
+        return false;  // the staged kernel serves the query
+    }
+    if (*st != BOLT_OK) return true;
+    GbParams& p = pl->prm;
+    if (cudaError_t e = smem_optin(sh.kernel, ctx); e != cudaSuccess) {
+        *st = cuda_fail(ctx, e, "smem_optin");
+        return true;
+    }
+    pl->grid = q.grid_a;
+    kernel_mark_begin(ctx, flags, s);
+    sh.kernel<<<q.grid_a, sh.block, sh.smem, s>>>(p, q);
+    kernel_mark_end(ctx, flags, s);
+    ctx->last_launches++;
+    const cudaError_t e = cudaGetLastError();
+    *st = e == cudaSuccess ? BOLT_OK : cuda_fail(ctx, e, "streaming GROUP BY launch");
+    return true;
+}
+
+// Plans and launches passes A, B1, S, B2 and C for one query whose compact
+// group array, words and finalize buffers are set up (see the header).
+bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags, int pbits_override) {
+    GbParams& p = pl->prm;
+    GbFinal& fin = pl->fin;
+    GbPart q{};
+    LeanShape sh;
+    bolt_status st0 = lean_setup<MISS_SPILL>(ctx, pl, q, sh);
+    if (st0 != BOLT_OK) return st0;
+    const LeanKernel kA = sh.kernel;
+    const ReduceKernel kC = reduce_kernel_for(p.spec);
+    if (!kC) return fail(ctx, BOLT_DECLINE, "GROUP BY: no partitioned-tier kernel for this layout");
+    const uint64_t groups = std::max<uint64_t>(pl->groups_hint, 1024);
+    // Partitions: about RED_GROUPS expected groups each.
+    int pbits = pbits_override > 0 ? pbits_override
+                                   : ceil_log2_u64((groups + GB_PART_RED_GROUPS - 1) / GB_PART_RED_GROUPS);
+    pbits = std::max(6, std::min(pbits, GB_PART_MAX_PBITS));
+    q.pbits = pbits;
+    const uint32_t P = 1u << pbits;
+    // The drained stages hold the partial-record histogram (P words).
+    if ((size_t)p.n_stages * p.stage_bytes < (size_t)P * 4)
+        return fail(ctx, BOLT_DECLINE, "GROUP BY: partitioned tier stages smaller than the histogram");
+    const int G = q.grid_a;
+    const uint32_t T = p.tile_rows;
+    const int nw = sh.block / 32 - 1;
     // Segment capacity: the most rows one CTA can see (its whole tiles plus
     // its share of the tail rows).
     const uint64_t ntiles = p.n_rows / T;
@@ -858,6 +1016,8 @@ bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t f
     q.seg_stride = ((ntiles + G - 1) / G) * T + ((rem + tail_step - 1) / tail_step) * (uint64_t)nw * 32;
     q.seg_stride = (q.seg_stride + 31) & ~31ull;
     const int W = p.sslot_words;
+    const size_t budget = (size_t)std::max(ctx->max_smem_optin - 1024, 0);
+    const size_t entry = 8ull * (size_t)p.sslot_words;
     // Pass C table: 4x the expected groups per partition, at most the
     // shared memory; admission up to 7/8 of it.
     const uint64_t per_part = (groups + P - 1) / P;
@@ -891,7 +1051,7 @@ bolt_status gb_part_launch(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t f
     // The profiled interval spans the aggregation kernels (A to C).
     BOLT_CUDA(ctx, smem_optin(kA, ctx));
     kernel_mark_begin(ctx, flags, s);
-    kA<<<G, block, smemA, s>>>(p, q);
+    kA<<<G, sh.block, sh.smem, s>>>(p, q);
     BOLT_CUDA(ctx, cudaGetLastError());
     BOLT_CUDA(ctx, smem_optin(gb_part_count_kernel, ctx));
     gb_part_count_kernel<<<G, 1024, (size_t)P * 4, s>>>(q);

@@ -50,8 +50,18 @@ struct alignas(16) GbPart {
     ull* dpar;            // partial records in partition order
 };
 
+// Whether the streaming kernel (compiled key / predicate / state layouts over
+// dense, 16-byte aligned columns of 4M+ rows) serves this planned query.
+bool gb_lean_applies(const GbPlan& pl, uint32_t flags);
+
 // Whether the partitioned tier serves this planned query.
 bool gb_part_applies(const bolt_ctx* ctx, const GbPlan& pl, uint32_t flags);
+
+// The global-table tier's aggregation through the streaming kernel (misses
+// go to the global hash table, set up in prm). Returns false when the
+// streaming kernel does not serve the query (the caller launches the staged
+// or register kernel); otherwise *st is the launch status.
+bool gb_lean_global(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_t flags, bolt_status* st);
 
 // Enqueues passes A, B1, S, B2 and C of one query whose compact group array
 // (prm.gtab, cap + 2 slots with the two special slots zeroed), words and

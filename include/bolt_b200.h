@@ -92,7 +92,8 @@ typedef struct bolt_ctx bolt_ctx;
 #define BOLT_FLAG_NO_TUNE      0x10u /* GROUP BY: ignore the context's autotuned choices */
 #define BOLT_FLAG_KERNEL_REGS  0x20u /* GROUP BY: aggregate with the register-tile kernel; compaction: per-element
                                        copies instead of bulk-staged tiles (testing) */
-#define BOLT_FLAG_KERNEL_STAGED 0x40u /* GROUP BY: aggregate with the staged kernel where it applies (testing) */
+#define BOLT_FLAG_KERNEL_STAGED 0x40u /* GROUP BY: aggregate with the generic staged kernel where it applies, not
+                                        the streaming kernel compiled for the query's layout (testing) */
 #define BOLT_FLAG_NO_PART      0x80u /* GROUP BY: never use the hash-partitioned tier (global hash table instead) */
 #define BOLT_FLAG_FORCE_PART   0x100u /* GROUP BY: use the hash-partitioned tier wherever it applies, whatever the
                                         groups hint (testing) */
