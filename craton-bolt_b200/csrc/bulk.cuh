@@ -78,4 +78,10 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
+// Bulk prefetch of `bytes` (a multiple of 16; 16-byte aligned start) of this
+// GPU's memory into the L2, completing asynchronously with no mbarrier.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 }  // namespace bolt

@@ -666,7 +666,17 @@ __global__ void __launch_bounds__(512) gb_part_reduce_kernel(const __grid_consta
     }
     __syncthreads();
     uint32_t absbits = 0;
+    // The first partition's rows into L2 (the others are prefetched one
+    // partition ahead, below).
+    if (threadIdx.x == 0 && blockIdx.x < P) {
+        const uint32_t rb = q.base_raw[blockIdx.x], re = q.base_raw[blockIdx.x + 1];
+        if (re > rb) bulk_prefetch_l2(q.drec + (uint64_t)rb * REC_WORDS, (re - rb) * REC_WORDS * 8u);
+    }
     for (uint32_t part = blockIdx.x; part < P; part += gridDim.x) {
+        if (threadIdx.x == 0 && part + gridDim.x < P) {
+            const uint32_t nb = q.base_raw[part + gridDim.x], ne = q.base_raw[part + gridDim.x + 1];
+            if (ne > nb) bulk_prefetch_l2(q.drec + (uint64_t)nb * REC_WORDS, (ne - nb) * REC_WORDS * 8u);
+        }
         // Partial states of the pass-A shared tables.
         const uint32_t pb = q.base_par[part], pe = q.base_par[part + 1];
         for (uint32_t j = pb + threadIdx.x; j < pe; j += blockDim.x) {
@@ -685,22 +695,34 @@ __global__ void __launch_bounds__(512) gb_part_reduce_kernel(const __grid_consta
                 merge_words_smem(w + at, k, rec[at], two ? rec[at + 1] : 0ull, true);
             }
         }
-        // Spilled rows.
+        // Spilled rows, RU per thread loaded before any is folded.
+        constexpr int RU = 4;
         const uint32_t rb = q.base_raw[part], re = q.base_raw[part + 1];
-        for (uint32_t j = rb + threadIdx.x; j < re; j += blockDim.x) {
-            const ulonglong2* rec = reinterpret_cast<const ulonglong2*>(q.drec + (uint64_t)j * REC_WORDS);
-            const ulonglong2 r0 = __ldcs(rec), r1 = __ldcs(rec + 1);
-            const ull fw[GB_PART_MAX_FIELDS] = {r0.y, r1.x, r1.y};
-            const int sl = r_find_insert(sk, q.red_log2, r0.x, &s_fill, q.red_fill);
-            if (sl < 0) {
-                atomicOr(p.status, ST_FLAG_SPILL);
-                continue;
-            }
-            ull c0[SP::n], c1[SP::n];
-            row_contrib<SP>(p, q, fw, c0, c1, absbits);
-            ull* w = sw + (ull)sl * SW - 1;
+        for (uint32_t j0 = rb + threadIdx.x; j0 < re; j0 += blockDim.x * RU) {
+            ulonglong2 r0[RU], r1[RU];
 #pragma unroll
-            for (int s = 0; s < SP::n; ++s) merge_words_smem(w + p.st[s].sword, SP::kind(s), c0[s], c1[s], true);
+            for (int u = 0; u < RU; ++u) {
+                const uint32_t j = j0 + (uint32_t)u * blockDim.x;
+                const ulonglong2* rec = reinterpret_cast<const ulonglong2*>(q.drec + (uint64_t)j * REC_WORDS);
+                r0[u] = j < re ? __ldcs(rec) : make_ulonglong2(0, 0);
+                r1[u] = j < re ? __ldcs(rec + 1) : make_ulonglong2(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < RU; ++u) {
+                if (j0 + (uint32_t)u * blockDim.x >= re) break;
+                const ull fw[GB_PART_MAX_FIELDS] = {r0[u].y, r1[u].x, r1[u].y};
+                const int sl = r_find_insert(sk, q.red_log2, r0[u].x, &s_fill, q.red_fill);
+                if (sl < 0) {
+                    atomicOr(p.status, ST_FLAG_SPILL);
+                    continue;
+                }
+                ull c0[SP::n], c1[SP::n];
+                row_contrib<SP>(p, q, fw, c0, c1, absbits);
+                ull* w = sw + (ull)sl * SW - 1;
+#pragma unroll
+                for (int s = 0; s < SP::n; ++s)
+                    merge_words_smem(w + p.st[s].sword, SP::kind(s), c0[s], c1[s], true);
+            }
         }
         __syncthreads();
         // Drain: every occupied slot becomes one group of the compact array,
