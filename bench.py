@@ -8,7 +8,9 @@ high-cardinality two-key GROUP BY
 over 100,000,000 seeded synthetic rows ((a, b) int32 pairs of 10M Zipf(1.1)
 ranks, f int32 U[0,100), vd f64 N(0,1e3), vi int64 uniform).
 
-Other workloads (per-operator lines): groupby_plain (1M rows, 1024 keys),
+At N=1 the default line also carries an `operators` map: every other
+workload below at its full size with fewer repeats. Other workloads
+(per-operator lines): groupby_plain (1M rows, 1024 keys),
 join_groupby (10M-row build, 200M-row probe, Decimal128 SUM), sort_i64
 (256M int64 keys), sort_f32 (64M float32 keys with specials), compact
 (100M-row WHERE compaction), batch (4096 filter + GROUP BY queries,
@@ -248,8 +250,10 @@ class Ctx:
         nk = self.lib.bolt_ctx_kernel_times(self.eng._ctx, kt, 4096)
         return [kt[i] for i in range(nk)][-last:]
 
-    def timed(self, step, steps: int, warmup: int):
-        """Runs warmup + K async steps; returns (device ms, launches, kernel ms list, clocks)."""
+    def timed(self, step, steps: int, warmup: int, marks_per_step: int = 1):
+        """Runs warmup + K async steps; returns (device ms, launches, kernel ms
+        list of the timed steps' profiled kernels, clocks). marks_per_step:
+        profiled kernels per step (the kernel list holds the last K of them)."""
         torch = self.torch
         sampler = ClockSampler(self.local) if not self.args.no_clocks else ClockSampler(-1)
         sampler.start()
@@ -271,7 +275,7 @@ class Ctx:
         self.barrier()
         ms = self.max_over_ranks(e0.elapsed_time(e1))
         self.check("timed region")
-        kms = self.kernel_times(steps)
+        kms = self.kernel_times(steps * marks_per_step)
         sampler.stop()
         return ms, launches, kms, sampler.summary(t0, t1)
 
@@ -369,6 +373,7 @@ def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
     if c.args.tier == "part":
         return PART_KERNELS
     staged = rows >= (1 << 22)
+    lean = "gb_lean_kernel (streaming kernel compiled for the query's layout; misses to the global hash table)"
     if tuned:
         import tempfile
         with tempfile.NamedTemporaryFile("r", suffix=".txt") as f:
@@ -378,7 +383,7 @@ def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
             staged = int(lines[0][6]) > 0
             if len(lines[0]) >= 9 and int(lines[0][8]) == 1 and c.args.tier == "auto":
                 return PART_KERNELS
-    return "gb_staged_kernel" if staged else "gb_agg_kernel"
+    return lean if staged else "gb_agg_kernel"
 
 
 def cpu_rows_per_s_groupby(table_np: dict, dts: dict, group_by, aggs, where, n_sample: int, runs: int = 5):
@@ -496,9 +501,7 @@ def w_join_groupby(c: Ctx):
     dg = datagen()
     nb, npr = a.build_rows, a.probe_rows
     bt = dg.join_build(nb, seed=3)
-    chunks = [dg.join_probe(min(1 << 25, npr - s), nb, seed=3, start=s) for s in range(0, npr, 1 << 25)]
-    pt = {"fk": np.concatenate([x["fk"] for x in chunks]), "amount": np.concatenate([x["amount"] for x in chunks])}
-    del chunks
+    pt = join_probe_host(dg, npr, nb)
     bk = c.bolt.Column(torch.from_numpy(bt["k"]).to(c.dev), "i64")
     bg = c.bolt.Column(torch.from_numpy(bt["g"]).to(c.dev), "i32")
     pk = c.bolt.Column(torch.from_numpy(pt["fk"]).to(c.dev), "i64")
@@ -529,7 +532,7 @@ def w_join_groupby(c: Ctx):
         c.lib.bolt_hash_join_release(c.eng._ctx, t)
         return n_l
 
-    ms, launches, kms, clocks = c.timed(step, a.steps, a.warmup)
+    ms, launches, kms, clocks = c.timed(step, a.steps, a.warmup, marks_per_step=2)
     # kernel times alternate build, probe-aggregate: the probe side dominates
     probe_k = kms[1::2] if len(kms) >= 2 else kms
     alg_probe = npr * 24
@@ -552,6 +555,25 @@ def w_join_groupby(c: Ctx):
     return line
 
 
+def join_probe_host(dg, npr: int, nb: int) -> dict:
+    """The probe side (fk, amount) generated in 32M-row chunks on every host
+    thread (each chunk is a pure function of its row range)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    fk = np.empty(npr, np.int64)
+    amount = np.empty((npr, 2), np.int64)
+
+    def part(s):
+        ch = dg.join_probe(min(1 << 25, npr - s), nb, seed=3, start=s)
+        fk[s:s + len(ch["fk"])] = ch["fk"]
+        amount[s:s + len(ch["fk"])] = ch["amount"]
+
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        list(pool.map(part, range(0, npr, 1 << 25)))
+    return {"fk": fk, "amount": amount}
+
+
 # ---------------------------------------------------------------------------
 # Workloads: ORDER BY radix sort
 # ---------------------------------------------------------------------------
@@ -561,8 +583,8 @@ def w_sort(c: Ctx, kind: str):
     dg = datagen()
     if kind == "i64":
         n = a.sort_rows
-        keys = np.concatenate([dg.uniform_u64(4, 31, min(1 << 26, n - s), s).view(np.int64)
-                               for s in range(0, n, 1 << 26)])
+        keys = np.empty(n, np.int64)
+        dg._chunked(n, lambda a, b: keys.__setitem__(slice(a, b), dg.uniform_u64(4, 31, b - a, a).view(np.int64)))
         dt, kb, np_ = "i64", 8, 8
     else:
         n = a.sortf_rows
@@ -634,9 +656,23 @@ def w_compact(c: Ctx):
     alg = a.rows * FILTERED_BYTES * 1.5  # read all columns, write the ~50% kept
     kernel = ("compact_count_kernel + compact_scan_kernel + compact_bulk_kernel (two-pass form)"
               if a.rows >= (1 << 22) else "compact_bulk_kernel")
-    return base_line(c, ms, a.rows, alg, kms, kernel, "compact",
+    line = base_line(c, ms, a.rows, alg, kms, kernel, "compact",
                      {"workload": "WHERE f < 50 compaction of 5 columns (28 B/row), 100M rows", "rows": a.rows,
                       "l2": "inputs larger than L2"}, launches, clocks, "mixed")
+    if not a.no_cpu:
+        orc = oracle_mod()
+        ns = min(a.cpu_rows, a.rows)
+        host = {k: orc.HostCol(np.ascontiguousarray(v[:ns]), FILTERED_DT[k]) for k, v in data.items()}
+        orc.compact(host, where=[("f", "<", 50)])
+        times = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            orc.compact(host, where=[("f", "<", 50)])
+            times.append(time.perf_counter() - t0)
+        line["cpu_baseline"] = {"value": ns / statistics.median(times), "unit": "rows/s", "cores": 1, "kind": "port",
+                                "sample": f"first {ns} rows, the oracle's order-preserving filter (selected row "
+                                          "indices), 1 thread; median of 5 runs after 1 warm-up"}
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -788,6 +824,47 @@ WORKLOADS = {"groupby_filtered": w_groupby_filtered, "groupby_plain": w_groupby_
 
 
 # ---------------------------------------------------------------------------
+# Every other operator, summarised inside the default line
+# ---------------------------------------------------------------------------
+OPERATORS = ["groupby_plain", "join_groupby", "sort_i64", "sort_f32", "compact", "batch"]
+OP_KEYS = ("value", "unit", "ms_per_step", "steps", "warmup", "dtype", "config", "roofline", "cpu_baseline", "e2e",
+           "gpu_launches", "clocks", "note", "batched_qps", "one_at_a_time_qps", "speedup", "latency_us",
+           "results_equal_alone_vs_mix", "rows_per_s_batched")
+
+
+def run_operators(c: Ctx) -> dict:
+    """Each other workload at its own full size with fewer repeats (at most 5
+    timed steps after 3 warm-up steps, one end-to-end step), summarised as a
+    sub-line of the default line's `operators` map."""
+    import copy
+
+    import torch
+
+    saved = c.args
+    out = {}
+    for name in OPERATORS:
+        a = copy.copy(saved)
+        a.steps, a.warmup, a.e2e_steps = min(saved.steps, 5), 3, 1
+        c.args = a
+        progress(f"operator {name}")
+        try:
+            line = WORKLOADS[name](c)
+            d = {k: line[k] for k in OP_KEYS if k in line}
+            if "small_query_mix" in line:
+                sm = line["small_query_mix"]
+                d["small_query_mix"] = {k: sm[k] for k in ("batched_qps", "one_at_a_time_qps", "speedup", "latency_us",
+                                                           "results_equal_alone_vs_mix", "workload") if k in sm}
+            out[name] = d
+        except Exception as e:  # noqa: BLE001  (one failing operator must not hide the others)
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:400]}
+        finally:
+            c.args = saved
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Reference arm
 # ---------------------------------------------------------------------------
 def run_reference(args):
@@ -856,6 +933,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the GROUP BY autotuner")
     ap.add_argument("--tuning", default=None, help="load GROUP BY launch choices from this file instead of tuning")
     ap.add_argument("--save-tuning", default=None, help="write the GROUP BY launch choices to this file")
+    ap.add_argument("--no-operators", action="store_true",
+                    help="default workload: skip the other operators' summary lines (the `operators` map)")
     ap.add_argument("--tier", default="auto", choices=["auto", "global", "part"],
                     help="GROUP BY tier: the library's choice, shared-memory + global hash table, hash-partitioned")
     args = ap.parse_args()
@@ -870,6 +949,8 @@ def main():
     c = Ctx(args)
     progress("context ready")
     line = WORKLOADS[args.workload](c)
+    if args.workload == "groupby_filtered" and c.world == 1 and not args.no_operators:
+        line["operators"] = run_operators(c)
     if c.rank == 0:
         print(json.dumps(line), flush=True)
     c.eng.close()
