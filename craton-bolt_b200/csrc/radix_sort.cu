@@ -6,13 +6,14 @@
 //   * one histogram kernel reads the keys once and counts all digit
 //     positions of every segment (8-bit digits: 4 passes for 32-bit keys,
 //     8 for 64-bit);
-//   * one kernel per digit: tiles of 3072 (64-bit) or 5120 (32-bit) keys are
-//     taken in arrival order
-//     from a flattened (segment, tile) list, ranked per warp with
-//     __match_any_sync (stable: element order within a warp's segment of the
-//     tile, warps in order), their digit counts chained across the segment's
-//     tiles with decoupled look-back (Merrill & Garland 2016), staged
-//     digit-sorted in shared memory and written out in coalesced runs;
+//   * one kernel per digit: tiles of 4096 (64-bit) or 5120 (32-bit) keys are
+//     taken in arrival order from a flattened (segment, tile) list; each
+//     tile's digit counts (per-warp shared atomics) are published first and
+//     chained across the segment's tiles with decoupled look-back (Merrill &
+//     Garland 2016); the keys are ranked per warp (stable: element order
+//     within a warp's part of the tile, warps in order; the lanes holding one
+//     digit find each other through a shared mask word), staged digit-sorted
+//     in shared memory and written out in coalesced runs;
 //   * a digit where all of a segment's keys fall in one bucket is skipped
 //     for that segment on the device;
 //   * the first pass applies the key transform of gpu_sort.rs:1089-1163 to
@@ -31,7 +32,7 @@ constexpr int SORT_BLOCK = 256;
 // Keys per thread in a pass: 32-bit keys leave registers and shared memory
 // for larger tiles (fewer tiles to chain, more independent loads per thread).
 constexpr int SORT_ITEMS_32 = 20;
-constexpr int SORT_ITEMS_64 = 12;
+constexpr int SORT_ITEMS_64 = 16;
 constexpr int SORT_TILE_MIN = SORT_BLOCK * SORT_ITEMS_64;
 constexpr int HIST_CHUNK = 16384;
 constexpr uint32_t LB_AGG = 1u << 30;
@@ -86,36 +87,42 @@ struct SortArgs {
     uint32_t* status;
 };
 
-__device__ __forceinline__ uint32_t sort_key_u32(int src, const void* p, uint64_t r, int desc) {
-    uint32_t k;
+// Order-preserving unsigned image of a key's raw bits: one load serves
+// every source type, the transform follows (so unrolled loads stay in flight
+// together).
+__device__ __forceinline__ uint32_t order_key(int src, uint32_t b, int desc) {
+    uint32_t k = b;
     if (src == SRC_I32) {
-        k = (uint32_t)__ldg((const int32_t*)p + r) ^ 0x80000000u;
+        k = b ^ 0x80000000u;
     } else if (src == SRC_F32) {
-        uint32_t b = canon_f32_bits(__ldg((const float*)p + r));
-        k = b ^ ((uint32_t)(((int32_t)b) >> 31) | 0x80000000u);
-    } else {
-        k = __ldg((const uint32_t*)p + r);
+        const uint32_t c = canon_f32_bits(__uint_as_float(b));
+        k = c ^ ((uint32_t)(((int32_t)c) >> 31) | 0x80000000u);
     }
     return desc ? ~k : k;
 }
-
-__device__ __forceinline__ ull sort_key_u64(int src, const void* p, uint64_t r, int desc) {
-    ull k;
-    if (src == SRC_I64) k = (ull)__ldg((const ll*)p + r) ^ 0x8000000000000000ull;
-    else if (src == SRC_F64) k = f64_order_key(__ldg((const double*)p + r));
-    else k = __ldg((const ull*)p + r);
+__device__ __forceinline__ ull order_key(int src, ull b, int desc) {
+    ull k = b;
+    if (src == SRC_I64) k = b ^ 0x8000000000000000ull;
+    else if (src == SRC_F64) k = f64_order_key(__longlong_as_double((long long)b));
     return desc ? ~k : k;
 }
 
 template <typename K>
-__device__ __forceinline__ K load_key(int src, const void* p, uint64_t r, int desc);
-template <>
-__device__ __forceinline__ uint32_t load_key<uint32_t>(int src, const void* p, uint64_t r, int desc) {
-    return sort_key_u32(src, p, r, desc);
+__device__ __forceinline__ K raw_key(const void* p, uint64_t r) {
+    return __ldg(reinterpret_cast<const K*>(p) + r);
 }
-template <>
-__device__ __forceinline__ ull load_key<ull>(int src, const void* p, uint64_t r, int desc) {
-    return sort_key_u64(src, p, r, desc);
+
+// Digit of a key at bit offset `shift` (a multiple of 8): a digit never
+// straddles the two 32-bit halves of a 64-bit key, so it is taken from the
+// half that holds it.
+template <typename K>
+__device__ __forceinline__ uint32_t digit_of(K k, int shift) {
+    if constexpr (sizeof(K) == 8) {
+        const uint32_t h = shift >= 32 ? (uint32_t)(k >> 32) : (uint32_t)k;
+        return (h >> (shift & 31)) & 0xFFu;
+    } else {
+        return ((uint32_t)k >> shift) & 0xFFu;
+    }
 }
 
 __device__ __forceinline__ void st_volatile_u32(uint32_t* p, uint32_t v) {
@@ -161,11 +168,21 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(SortArgs a) {
         for (int i = threadIdx.x; i < NP * 256; i += blockDim.x) h[i] = 0;
         __syncthreads();
         const uint64_t c1 = c0 + HIST_CHUNK < n ? c0 + HIST_CHUNK : n;
-        for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-            const uint64_t r = a.indirect ? d.payload_in[i] : i;
-            const K k = load_key<K>(a.src, d.keys, r, a.desc);
+        for (uint64_t i0 = c0 + threadIdx.x; i0 < c1; i0 += 4 * blockDim.x) {
+            K raw[4];
 #pragma unroll
-            for (int p = 0; p < NP; ++p) atomicAdd(&h[p * 256 + (uint32_t)((k >> (8 * p)) & 0xFF)], 1u);
+            for (int u = 0; u < 4; ++u) {
+                const uint64_t i = i0 + (uint64_t)u * blockDim.x;
+                raw[u] = 0;
+                if (i < c1) raw[u] = raw_key<K>(d.keys, a.indirect ? d.payload_in[i] : i);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (i0 + (uint64_t)u * blockDim.x >= c1) continue;
+                const K k = order_key(a.src, raw[u], a.desc);
+#pragma unroll
+                for (int p = 0; p < NP; ++p) atomicAdd(&h[p * 256 + digit_of<K>(k, 8 * p)], 1u);
+            }
         }
         __syncthreads();
         uint32_t* gh = a.hist + (uint64_t)sg * NP * 256;
@@ -216,19 +233,22 @@ __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, in
     constexpr int SORT_ITEMS = KeyTraits<K>::ITEMS;
     constexpr int SORT_TILE = KeyTraits<K>::TILE;
     __shared__ uint32_t s_item;
-    __shared__ uint32_t warp_hist[NW][256];
-    __shared__ uint32_t tile_off[256];
-    __shared__ uint32_t gstart[256];
-    __shared__ uint32_t wsum[8];
-    // Staged tile: keys, payloads and the digit of every position
-    // (3 CTAs of 256 threads per SM).
+    __shared__ uint32_t warp_pos[NW][256];  // per-warp digit counts, then each warp's next staged position
+    __shared__ uint32_t peer_bits[NW][256];  // per-warp lane masks of the lanes holding a digit
+    __shared__ uint32_t gdelta[256];         // global position of staged position 0, per digit
+    __shared__ uint32_t wsum[NW];
+    // Staged tile: keys (or, in the last pass, the digit of every position)
+    // and payloads (3 CTAs of 256 threads per SM).
     extern __shared__ __align__(16) unsigned char dyn[];
     K* stage_key = reinterpret_cast<K*>(dyn);
     uint32_t* stage_pay = reinterpret_cast<uint32_t*>(dyn + sizeof(K) * SORT_TILE);
     uint8_t* stage_dig = dyn + (sizeof(K) + 4) * SORT_TILE;
 
     if (threadIdx.x == 0) s_item = atomicAdd(&a.tile_ctr[p], 1u);
-    for (int i = threadIdx.x; i < NW * 256; i += SORT_BLOCK) (&warp_hist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < NW * 256; i += SORT_BLOCK) {
+        (&warp_pos[0][0])[i] = 0;
+        (&peer_bits[0][0])[i] = 0;
+    }
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= a.total_items) return;
@@ -252,91 +272,119 @@ __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, in
     uint32_t* lb_next = a.lookback + (uint64_t)((kidx + 1) & 1) * a.lb_stride;
 
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* peers_w = peer_bits[w];
     const uint64_t seg0 = (uint64_t)tile * SORT_TILE + (uint64_t)w * 32 * SORT_ITEMS;
     const int shift = 8 * p;
+    const bool full = (uint64_t)(tile + 1) * SORT_TILE <= n;
     K key[SORT_ITEMS];
     uint32_t pay[SORT_ITEMS];
-    uint32_t rank[SORT_ITEMS];
+    if (first) {
+        // Raw key bits first (all loads in flight), then the transform.
+        if (a.indirect) {
 #pragma unroll
-    for (int j = 0; j < SORT_ITEMS; ++j) {
-        const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
-        key[j] = 0;
-        pay[j] = 0;
-        if (e < n) {
-            if (first) {
-                pay[j] = d.payload_in ? d.payload_in[e] : (uint32_t)e;
-                key[j] = load_key<K>(a.src, d.keys, a.indirect ? pay[j] : e, a.desc);
-            } else {
+            for (int j = 0; j < SORT_ITEMS; ++j) {
+                const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
+                pay[j] = (full || e < n) ? d.payload_in[e] : 0u;
+            }
+#pragma unroll
+            for (int j = 0; j < SORT_ITEMS; ++j) {
+                const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
+                key[j] = (full || e < n) ? raw_key<K>(d.keys, pay[j]) : (K)0;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < SORT_ITEMS; ++j) {
+                const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
+                key[j] = 0;
+                pay[j] = 0;
+                if (full || e < n) {
+                    pay[j] = d.payload_in ? d.payload_in[e] : (uint32_t)e;
+                    key[j] = raw_key<K>(d.keys, e);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < SORT_ITEMS; ++j) key[j] = order_key(a.src, key[j], a.desc);
+    } else {
+#pragma unroll
+        for (int j = 0; j < SORT_ITEMS; ++j) {
+            const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
+            key[j] = 0;
+            pay[j] = 0;
+            if (full || e < n) {
                 key[j] = kin[e];
                 pay[j] = pin[e];
             }
         }
     }
-    // Stable per-warp ranking in element order.
+    // Early counts: per-warp digit histograms from shared atomics, so the
+    // tile's counts are published before the (longer) ranking and later
+    // tiles' look-backs find them sooner.
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
         const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
-        const bool valid = e < n;
-        const uint32_t dg = valid ? (uint32_t)(key[j] >> shift) & 0xFFu : 0u;
-        // Lanes holding the same digit: one ballot per digit bit.
-        uint32_t peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-        for (int bit = 0; bit < 8; ++bit) {
-            const uint32_t on = (dg >> bit) & 1u;
-            const uint32_t bal = __ballot_sync(0xffffffffu, on);
-            peers &= on ? bal : ~bal;
-        }
-        const int leader = valid ? 31 - __clz(peers) : (int)lane;
-        uint32_t b = 0;
-        if (valid && (int)lane == leader) {
-            b = warp_hist[w][dg];
-            warp_hist[w][dg] = b + __popc(peers);
-        }
-        b = __shfl_sync(0xffffffffu, b, leader);
-        rank[j] = valid ? b + __popc(peers & lanemask_lt()) : 0u;
-        __syncwarp();
+        if (full || e < n) atomicAdd(&warp_pos[w][digit_of<K>(key[j], shift)], 1u);
     }
     __syncthreads();
-
-    // Per-digit warp offsets and tile counts; the tile's counts are published
-    // at once so later tiles can look back past it.
     const uint32_t dg_me = threadIdx.x;  // SORT_BLOCK == 256: one digit per thread
+    uint32_t cnt[NW];
     uint32_t run = 0;
+#pragma unroll
+    for (int ww = 0; ww < NW; ++ww) {
+        cnt[ww] = warp_pos[ww][dg_me];
+        run += cnt[ww];
+    }
+    st_volatile_u32(lb + (uint64_t)item * 256 + dg_me, (tile == 0 ? LB_INC : LB_AGG) | run);
+    // Exclusive scan of the tile's digit counts; each warp's first staged
+    // position per digit follows.
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    uint32_t tile_off = x - run;
+    for (int i = 0; i < w; ++i) tile_off += wsum[i];
     {
+        uint32_t off = tile_off;
 #pragma unroll
         for (int ww = 0; ww < NW; ++ww) {
-            const uint32_t c = warp_hist[ww][dg_me];
-            warp_hist[ww][dg_me] = run;
-            run += c;
+            warp_pos[ww][dg_me] = off;
+            off += cnt[ww];
         }
-        st_volatile_u32(lb + (uint64_t)item * 256 + dg_me, (tile == 0 ? LB_INC : LB_AGG) | run);
-        // Exclusive scan of the tile's digit counts.
-        uint32_t x = run;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) wsum[w] = x;
-        __syncthreads();
-        uint32_t wp = 0;
-        for (int i = 0; i < w; ++i) wp += wsum[i];
-        tile_off[dg_me] = wp + x - run;
     }
     __syncthreads();
 
-    // Stage the tile digit-sorted (keys unless this is the last pass,
-    // payloads, digits); the registers are free for the look-back.
+    // Stable ranking in element order (items in order, lanes in order within
+    // an item), straight to the staged position. The lanes holding the same
+    // digit find each other through one shared mask word per (warp, digit);
+    // the highest of them advances the warp's position for that digit.
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; ++j) {
         const uint64_t e = seg0 + (uint64_t)j * 32 + lane;
-        if (e < n) {
-            const uint32_t dg = (uint32_t)(key[j] >> shift) & 0xFFu;
-            const uint32_t pos = tile_off[dg] + warp_hist[w][dg] + rank[j];
-            stage_dig[pos] = (uint8_t)dg;
+        const bool valid = full || e < n;
+        const uint32_t dg = digit_of<K>(key[j], shift);
+        if (valid) atomicOr(&peers_w[dg], 1u << lane);
+        __syncwarp();
+        const uint32_t peers = valid ? peers_w[dg] : (1u << lane);
+        __syncwarp();
+        const int leader = 31 - __clz(peers);
+        uint32_t b = 0;
+        if (valid && lane == leader) {
+            peers_w[dg] = 0;
+            b = warp_pos[w][dg];
+            warp_pos[w][dg] = b + __popc(peers);
+        }
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (valid) {
+            const uint32_t pos = b + __popc(peers & lanemask_lt());
             if (kout) stage_key[pos] = key[j];
+            else stage_dig[pos] = (uint8_t)dg;  // the last pass stages no keys
             stage_pay[pos] = pay[j];
         }
+        __syncwarp();
     }
 
     // Look back over the segment's earlier tiles, LB_WINDOW words in flight
@@ -348,16 +396,16 @@ __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, in
             const int64_t t_end = (int64_t)d.item_begin;
             uint32_t spins = 0;
             while (t >= t_end) {
-                const int cnt = (t - t_end + 1) < LB_WINDOW ? (int)(t - t_end + 1) : LB_WINDOW;
+                const int cnt_w = (t - t_end + 1) < LB_WINDOW ? (int)(t - t_end + 1) : LB_WINDOW;
                 uint32_t v[LB_WINDOW];
 #pragma unroll
                 for (int i = 0; i < LB_WINDOW; ++i)
-                    v[i] = i < cnt ? ld_volatile_u32(lb + (uint64_t)(t - i) * 256 + dg_me) : 0u;
+                    v[i] = i < cnt_w ? ld_volatile_u32(lb + (uint64_t)(t - i) * 256 + dg_me) : 0u;
                 int used = 0;
                 bool done = false, stalled = false;
 #pragma unroll
                 for (int i = 0; i < LB_WINDOW; ++i) {
-                    if (done || stalled || i >= cnt) continue;
+                    if (done || stalled || i >= cnt_w) continue;
                     const uint32_t st = v[i] >> 30;
                     if (st == 0) {
                         stalled = true;  // not published yet: poll again from here
@@ -380,22 +428,35 @@ __global__ void __launch_bounds__(SORT_BLOCK, 3) sort_pass_kernel(SortArgs a, in
             st_volatile_u32(lb + (uint64_t)item * 256 + dg_me, LB_INC | ((excl + run) & LB_VAL));
         }
         lb_next[(uint64_t)item * 256 + dg_me] = 0;
-        gstart[dg_me] = a.digit_base[((uint64_t)sg * KeyTraits<K>::NPASS + p) * 256 + dg_me] + excl;
+        // Positions fit in 32 bits (n < 2^30), so the difference wraps safely.
+        gdelta[dg_me] = a.digit_base[((uint64_t)sg * KeyTraits<K>::NPASS + p) * 256 + dg_me] + excl - tile_off;
     }
     __syncthreads();
 
     // Coalesced runs out of the staged tile.
     const uint64_t tb = (uint64_t)tile * SORT_TILE;
     const uint32_t tile_n = (uint32_t)((n - tb) < (uint64_t)SORT_TILE ? (n - tb) : (uint64_t)SORT_TILE);
-    for (uint32_t i = threadIdx.x; i < tile_n; i += SORT_BLOCK) {
-        const uint32_t dg = stage_dig[i];
-        const uint64_t g = (uint64_t)gstart[dg] + (i - tile_off[dg]);
-        if (g >= n) {  // only reachable after a look-back timeout
-            atomicOr(a.status, ST_FLAG_TIMEOUT);
-            continue;
+    const uint32_t n32 = (uint32_t)n;  // n < 2^30
+    if (kout) {
+        for (uint32_t i = threadIdx.x; i < tile_n; i += SORT_BLOCK) {
+            const K k = stage_key[i];
+            const uint32_t g = gdelta[digit_of<K>(k, shift)] + i;
+            if (g >= n32) {  // only reachable after a look-back timeout
+                atomicOr(a.status, ST_FLAG_TIMEOUT);
+                continue;
+            }
+            kout[g] = k;
+            pout[g] = stage_pay[i];
         }
-        if (kout) kout[g] = stage_key[i];
-        pout[g] = stage_pay[i];
+    } else {
+        for (uint32_t i = threadIdx.x; i < tile_n; i += SORT_BLOCK) {
+            const uint32_t g = gdelta[stage_dig[i]] + i;
+            if (g >= n32) {
+                atomicOr(a.status, ST_FLAG_TIMEOUT);
+                continue;
+            }
+            pout[g] = stage_pay[i];
+        }
     }
 }
 
