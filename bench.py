@@ -350,7 +350,7 @@ class PreparedCall:
         self.c, self.pq = c, pq
         self.ng = c.torch.zeros(1, dtype=c.torch.int64, device=c.dev)
         pq.out.n_groups_dev = self.ng.data_ptr()
-        self.flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE | tier_flags(c)
+        self.flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_KERNEL_TIMES | tier_flags(c)
 
     def __call__(self):
         c = self.c
@@ -368,11 +368,12 @@ PART_KERNELS = ("gb_spill_kernel + gb_part_count_kernel + gb_part_scan_kernel + 
 def agg_kernel_name(c: Ctx, rows: int, tuned: bool) -> str:
     """Which aggregation kernels the timed GROUP BY runs: the partitioned
     tier's five when --tier part or the tuning cache chooses it; else the
-    staged kernel when the tuning cache (or, untuned, the library's default
-    for inputs of 4M rows and more) chooses it, else the register-tile kernel."""
+    streaming kernel when the tuning cache (or, untuned, the library's default
+    for dense inputs of 256K rows and more) chooses it, else the register-tile
+    kernel."""
     if c.args.tier == "part":
         return PART_KERNELS
-    staged = rows >= (1 << 22)
+    staged = rows >= (1 << 18)
     lean = "gb_lean_kernel (streaming kernel compiled for the query's layout; misses to the global hash table)"
     if tuned:
         import tempfile
@@ -476,7 +477,7 @@ def w_groupby_plain(c: Ctx):
     call = PreparedCall(c, pq)
     ms, launches, kms, clocks = c.timed(call, a.steps, a.warmup)
     alg = n * 12
-    line = base_line(c, ms, n, alg, kms, "gb_agg_kernel", "groupby_plain",
+    line = base_line(c, ms, n, alg, kms, agg_kernel_name(c, n, False), "groupby_plain",
                      {"workload": "plain single-key GROUP BY: 1M rows, k int32 U[0,1024), v int64 U[-1e6,1e6]; "
                                   "SUM, COUNT(*), MIN, MAX", "rows": n, "groups_hint": 1024,
                       "l2": "12 MB input fits in L2: warm-L2 figure (launch-bound workload)"},
@@ -514,7 +515,7 @@ def w_join_groupby(c: Ctx):
     sm = abi.ColMut(s.data_ptr(), None, 4096, abi.DEC128, 2)
     cm = abi.ColMut(cnt.data_ptr(), None, 4096, abi.I64, 0)
     ng = C.c_uint64(0)
-    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE
+    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_KERNEL_TIMES
     bkv, bgv, pkv, amv = bk.view(), bg.view(), pk.view(), am.view()
 
     def step():
@@ -595,7 +596,7 @@ def w_sort(c: Ctx, kind: str):
     abi = importlib.import_module("craton_bolt_b200._abi")
     kv = col.view()
     pm = abi.ColMut(perm.data_ptr(), None, n, abi.U32, 0)
-    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE
+    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_KERNEL_TIMES
 
     def step():
         st = c.lib.bolt_radix_sort_perm(c.eng._ctx, C.byref(kv), 0, 0, C.byref(pm), flags,
@@ -643,7 +644,7 @@ def w_compact(c: Ctx):
                                        for k in names])
     pred = (abi.Pred * 1)(abi.Pred(names.index("f"), abi.CMP_CODES["<"], 50, 0.0))
     nout = C.c_uint64(0)
-    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_PROFILE
+    flags = c.bolt.FLAG_ASYNC | c.bolt.FLAG_KERNEL_TIMES
 
     def step():
         st = c.lib.bolt_compact(c.eng._ctx, views, len(names), pred, 1, muts, None, C.byref(nout), flags,

@@ -24,12 +24,13 @@ import torch
 
 from . import _abi
 from ._abi import (AGG_CODES, CMP_CODES, DTYPE_CODES, FLAG_ASYNC, FLAG_FORCE_GLOBAL, FLAG_FORCE_PART,
-                   FLAG_FORCE_SHMEM, FLAG_KERNEL_REGS, FLAG_KERNEL_STAGED, FLAG_NO_PART, FLAG_NO_TUNE, FLAG_PROFILE)
+                   FLAG_FORCE_SHMEM, FLAG_KERNEL_REGS, FLAG_KERNEL_STAGED, FLAG_KERNEL_TIMES, FLAG_NO_PART, FLAG_NO_TUNE,
+                   FLAG_PROFILE)
 
 __all__ = ["BoltError", "DeclineError", "SpillError", "TypeError_", "GpuCapacityError", "TimeoutError_",
            "CudaError", "PlanError", "Column", "Engine", "col", "GroupbyResult", "FLAG_ASYNC",
            "FLAG_PROFILE", "FLAG_FORCE_GLOBAL", "FLAG_FORCE_SHMEM", "FLAG_NO_TUNE", "FLAG_KERNEL_REGS",
-           "FLAG_KERNEL_STAGED", "FLAG_NO_PART", "FLAG_FORCE_PART", "lib", "PreparedGroupby",
+           "FLAG_KERNEL_STAGED", "FLAG_KERNEL_TIMES", "FLAG_NO_PART", "FLAG_FORCE_PART", "lib", "PreparedGroupby",
            "Server", "BatchGraph"]
 
 

@@ -39,6 +39,7 @@ FLAG_KERNEL_REGS = 0x20
 FLAG_KERNEL_STAGED = 0x40
 FLAG_NO_PART = 0x80
 FLAG_FORCE_PART = 0x100
+FLAG_KERNEL_TIMES = 0x200
 
 
 class ColView(C.Structure):

@@ -104,10 +104,11 @@ bolt_status call_end(bolt_ctx* ctx, uint32_t flags, cudaStream_t s);
 
 // Event pair around the dominant kernel of a profiled call.
 inline void kernel_mark_begin(bolt_ctx* ctx, uint32_t flags, cudaStream_t s) {
-    if ((flags & BOLT_FLAG_PROFILE) && ctx->kcount < bolt_ctx::KRING) cudaEventRecord(ctx->kev[2 * ctx->kcount], s);
+    if ((flags & (BOLT_FLAG_PROFILE | BOLT_FLAG_KERNEL_TIMES)) && ctx->kcount < bolt_ctx::KRING)
+        cudaEventRecord(ctx->kev[2 * ctx->kcount], s);
 }
 inline void kernel_mark_end(bolt_ctx* ctx, uint32_t flags, cudaStream_t s) {
-    if ((flags & BOLT_FLAG_PROFILE) && ctx->kcount < bolt_ctx::KRING) {
+    if ((flags & (BOLT_FLAG_PROFILE | BOLT_FLAG_KERNEL_TIMES)) && ctx->kcount < bolt_ctx::KRING) {
         cudaEventRecord(ctx->kev[2 * ctx->kcount + 1], s);
         ctx->kcount++;
     }

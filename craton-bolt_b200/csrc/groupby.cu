@@ -623,54 +623,150 @@ __global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fin
     }
 }
 
-// One CTA per small-table query (<= 8192 slots): compact + bitonic sort in
-// shared memory + emit.
-__global__ void __launch_bounds__(1024) gb_small_final_kernel(const GbFinal* fins) {
+// One CTA per small-table query (<= 8192 slots): compacts the occupied
+// slots, sorts their (order key, slot) pairs by key in shared memory and
+// emits the groups. The sort is a stable LSD radix sort over only the key
+// bytes that differ between the groups (two passes for keys below 2^16),
+// ranked per warp like the global radix sort.
+constexpr int SF_BLOCK = 512;
+constexpr int SF_NW = SF_BLOCK / 32;
+
+// Dynamic shared memory of gb_small_final_kernel for tables of `cap` slots:
+// two (key, slot) buffers of cap + 1 entries.
+inline size_t small_final_smem(uint64_t cap) { return (size_t)(cap + 1) * 2 * 12; }
+
+__device__ __forceinline__ void small_final_body(const GbFinal& f) {
     extern __shared__ __align__(16) ull sm[];
     __shared__ uint32_t s_n;
-    __shared__ __align__(16) GbFinal f;
-    load_final(f, fins + blockIdx.x);
+    __shared__ ull s_vary;
+    __shared__ uint32_t warp_pos[SF_NW][256];
+    __shared__ uint32_t wsum[8];
     const ull cap = 1ull << f.log2cap;
-    const uint32_t P = (uint32_t)cap * 2;  // power of two >= cap + 1
-    ull* key = sm;
-    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + P);
-    if (threadIdx.x == 0) s_n = 0;
+    const uint32_t M = (uint32_t)cap + 1;
+    ull* const key0 = sm;
+    ull* const key1 = sm + M;
+    uint32_t* const slot0 = reinterpret_cast<uint32_t*>(sm + 2 * (size_t)M);
+    uint32_t* const slot1 = slot0 + M;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_n = 0;
+        s_vary = 0;
+    }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i <= cap; i += blockDim.x) {
-        ull k = f.gtab[(ull)i * f.slot_words];
-        if (k == 0) continue;
-        uint32_t pos = atomicAdd(&s_n, 1u);
-        key[pos] = (i == cap ? ~0ull : ~k) ^ 0x8000000000000000ull;
-        slot[pos] = i;
+    // Occupied slots, 8 loads in flight per thread, one counter update per
+    // warp and load round.
+    constexpr int SF_U = 8;
+    for (uint32_t w0 = (threadIdx.x & ~31u) * SF_U; w0 <= cap; w0 += blockDim.x * SF_U) {  // (warp-uniform)
+        const uint32_t i0 = w0 + lane;
+        ull kk[SF_U];
+#pragma unroll
+        for (int u = 0; u < SF_U; ++u) {
+            const uint32_t i = i0 + 32u * u;
+            kk[u] = i <= cap ? f.gtab[(ull)i * f.slot_words] : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < SF_U; ++u) {
+            const uint32_t i = i0 + 32u * u;
+            const uint32_t m = __ballot_sync(0xffffffffu, kk[u] != 0);
+            if (m == 0) continue;
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&s_n, (uint32_t)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (kk[u] != 0) {
+                const uint32_t pos = base + __popc(m & lanemask_lt());
+                key0[pos] = (i == cap ? ~0ull : ~kk[u]) ^ 0x8000000000000000ull;
+                slot0[pos] = i;
+            }
+        }
     }
     __syncthreads();
     const uint32_t G = s_n;
-    uint32_t Pn = 1;
-    while (Pn < G) Pn <<= 1;
-    for (uint32_t i = G + threadIdx.x; i < Pn; i += blockDim.x) {
-        key[i] = ~0ull;
-        slot[i] = 0xFFFFFFFFu;
+    // Bits in which some group's key differs from the first one's.
+    if (G > 1) {
+        const ull k0 = key0[0];
+        ull v = 0;
+        for (uint32_t i = threadIdx.x; i < G; i += blockDim.x) v |= key0[i] ^ k0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicOr(&s_vary, v);
     }
     __syncthreads();
-    for (uint32_t k = 2; k <= Pn; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < Pn; i += blockDim.x) {
-                const uint32_t x = i ^ j;
-                if (x > i) {
-                    const bool asc = (i & k) == 0;
-                    const ull a = key[i], b = key[x];
-                    // Padding (slot ~0) always sorts last; keys are unique.
-                    const bool gt = (slot[i] == 0xFFFFFFFFu) ? (slot[x] != 0xFFFFFFFFu)
-                                  : (slot[x] == 0xFFFFFFFFu) ? false : a > b;
-                    if (gt == asc) {
-                        key[i] = b; key[x] = a;
-                        const uint32_t t = slot[i]; slot[i] = slot[x]; slot[x] = t;
-                    }
-                }
+    const ull vary = s_vary;
+    // Each warp ranks a contiguous run of the entries, so the passes keep
+    // the order of equal digits.
+    const uint32_t per = (((G + SF_NW - 1) / SF_NW) + 31) & ~31u;
+    const uint32_t lo = min((uint32_t)w * per, G), hi = min(lo + per, G);
+    int cur = 0;
+    for (int byte = 0; byte < 8; ++byte) {
+        if (((vary >> (8 * byte)) & 0xFFull) == 0) continue;  // (uniform over the CTA)
+        const int sh = 8 * byte;
+        const ull* ka = cur ? key1 : key0;
+        const uint32_t* sa = cur ? slot1 : slot0;
+        ull* kb = cur ? key0 : key1;
+        uint32_t* sb = cur ? slot0 : slot1;
+        for (int i = threadIdx.x; i < SF_NW * 256; i += blockDim.x) (&warp_pos[0][0])[i] = 0;
+        __syncthreads();
+        for (uint32_t i = lo + lane; i < hi; i += 32) atomicAdd(&warp_pos[w][(uint32_t)(ka[i] >> sh) & 0xFFu], 1u);
+        __syncthreads();
+        // Digit-major, then warp order: each warp's first position per digit.
+        uint32_t cnt[SF_NW];
+        uint32_t run = 0, x = 0;
+        if (threadIdx.x < 256) {
+#pragma unroll
+            for (int ww = 0; ww < SF_NW; ++ww) {
+                cnt[ww] = warp_pos[ww][threadIdx.x];
+                run += cnt[ww];
             }
-            __syncthreads();
+            x = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) wsum[w] = x;
         }
+        __syncthreads();
+        if (threadIdx.x < 256) {
+            uint32_t off = x - run;
+            for (int i = 0; i < w; ++i) off += wsum[i];
+#pragma unroll
+            for (int ww = 0; ww < SF_NW; ++ww) {
+                warp_pos[ww][threadIdx.x] = off;
+                off += cnt[ww];
+            }
+        }
+        __syncthreads();
+        for (uint32_t b0 = lo; b0 < hi; b0 += 32) {  // (warp-uniform)
+            const uint32_t i = b0 + lane;
+            const bool valid = i < hi;
+            const ull k = valid ? ka[i] : 0ull;
+            const uint32_t dg = (uint32_t)(k >> sh) & 0xFFu;
+            uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+            for (int bit = 0; bit < 8; ++bit) {
+                const uint32_t on = (dg >> bit) & 1u;
+                const uint32_t bal = __ballot_sync(0xffffffffu, on);
+                peers &= on ? bal : ~bal;
+            }
+            if (!valid) peers = 1u << lane;
+            const int leader = 31 - __clz(peers);
+            uint32_t bpos = 0;
+            if (valid && lane == leader) {
+                bpos = warp_pos[w][dg];
+                warp_pos[w][dg] = bpos + __popc(peers);
+            }
+            bpos = __shfl_sync(0xffffffffu, bpos, leader);
+            if (valid) {
+                const uint32_t pos = bpos + __popc(peers & lanemask_lt());
+                kb[pos] = k;
+                sb[pos] = sa[i];
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        cur ^= 1;
     }
+    const uint32_t* sorted = cur ? slot1 : slot0;
     const bool has_null = f.gtab[(cap + 1) * (ull)f.slot_words] != 0;
     const ull total = (ull)G + (has_null ? 1 : 0);
     if (threadIdx.x == 0) {
@@ -680,7 +776,19 @@ __global__ void __launch_bounds__(1024) gb_small_final_kernel(const GbFinal* fin
         if (total > f.out_cap) atomicOr(f.status, ST_FLAG_CAPACITY);
     }
     const ull lim = total < f.out_cap ? total : f.out_cap;
-    for (uint64_t o = threadIdx.x; o < lim; o += blockDim.x) emit_group(f, o, o < G ? slot[o] : cap + 1);
+    for (uint64_t o = threadIdx.x; o < lim; o += blockDim.x) emit_group(f, o, o < G ? sorted[o] : cap + 1);
+}
+
+// Several queries, one CTA each (descriptors in device memory).
+__global__ void __launch_bounds__(SF_BLOCK) gb_small_final_kernel(const GbFinal* fins) {
+    __shared__ __align__(16) GbFinal f;
+    load_final(f, fins + blockIdx.x);
+    small_final_body(f);
+}
+
+// One query, its descriptor passed by value (no upload before the launch).
+__global__ void __launch_bounds__(SF_BLOCK) gb_small_final1_kernel(const __grid_constant__ GbFinal f) {
+    small_final_body(f);
 }
 
 // ---------------------------------------------------------------------------
@@ -1122,15 +1230,17 @@ bolt_status gb_plan(bolt_ctx* ctx, const bolt_groupby_desc* d, const bolt_groupb
     pl->groups_hint = hint;
     // Autotuned choices for this query shape, if any (bolt_groupby_autotune).
     pl->shape = gb_shape_key(p, n, hint);
-    // Untuned default: the register kernel for small inputs, the staged
-    // kernel (2 chunks per consumer warp) from 4M rows, where its pipeline
-    // fills.
+    // Untuned default: the register kernel for small inputs; from 256K rows
+    // the streaming kernel compiled for the query's layout where it applies
+    // (measured faster from there: 1M rows, 1,024 groups 0.071 -> 0.058 ms
+    // per query), else the staged kernel (2 chunks per consumer warp) from
+    // 4M rows, where its pipeline fills.
     // Shared-tier admission cap in eighths of the table: half full when the
     // expected groups fit in it; 3/8 when they outnumber it, so keys that miss
     // meet an empty slot sooner (shorter divergent probe loops; measured
     // 3.05 -> 2.95 ms at 100M rows and 3.28M groups).
     const int fill = (hint && hint <= 1024) ? 4 : 3;
-    bolt_ctx::GbTune tn{512, 1, 0, 1, fill, n >= (1ull << 22) ? 2 : 0, 0.0};
+    bolt_ctx::GbTune tn{512, 1, 0, 1, fill, n >= GB_LEAN_MIN_ROWS ? 2 : 0, 0.0};
     if (!(flags & BOLT_FLAG_NO_TUNE)) {
         auto it = ctx->tune.find(pl->shape);
         if (it != ctx->tune.end()) tn = it->second;
@@ -1303,7 +1413,8 @@ static bolt_status gb_agg_one(bolt_ctx* ctx, GbPlan* pl, cudaStream_t s, uint32_
     size_t smem = (size_t)pl->smem_entries * 8ull * (size_t)p.sslot_words;
     const uint64_t tile = (uint64_t)pl->block * pl->u;
     GbStagedLaunch stg;
-    const bool staged = gb_staged_layout(ctx, *pl, &stg);
+    const bool staged = (p.n_rows >= GB_STAGED_MIN_ROWS || (flags & BOLT_FLAG_KERNEL_STAGED)) &&
+                        gb_staged_layout(ctx, *pl, &stg);
     AggKernel kfn;
     int block = pl->block;
     uint64_t tiles;
@@ -1428,14 +1539,18 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
             large_q.push_back(q);
         }
     }
-    if (!small.empty()) {
+    if (small.size() == 1) {
+        BOLT_CUDA(ctx, smem_optin(gb_small_final1_kernel, ctx));
+        gb_small_final1_kernel<<<1, SF_BLOCK, small_final_smem(small_cap), s>>>(small[0]);
+        ctx->last_launches++;
+    } else if (!small.empty()) {
         GbFinal* d_f = (GbFinal*)arena_alloc(ctx, sizeof(GbFinal) * small.size());
         if (!d_f) return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
         bolt_status st = stage_upload(ctx, s, d_f, small.data(), sizeof(GbFinal) * small.size());
         if (st != BOLT_OK) return st;
-        const size_t fsm = (size_t)small_cap * 2 * 12;
+        const size_t fsm = small_final_smem(small_cap);
         BOLT_CUDA(ctx, smem_optin(gb_small_final_kernel, ctx));
-        gb_small_final_kernel<<<(unsigned)small.size(), 1024, fsm, s>>>(d_f);
+        gb_small_final_kernel<<<(unsigned)small.size(), SF_BLOCK, fsm, s>>>(d_f);
         ctx->last_launches++;
     }
     if (!large_q.empty()) {
@@ -2020,10 +2135,10 @@ extern "C" bolt_status bolt_groupby_noalloc(const bolt_groupby_desc* desc, bolt_
             if (cudaGetLastError() != cudaSuccess)
                 return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: aggregation launch failed");
         }
-        const size_t fsm = (size_t)pl.cap * 2 * 12;
+        const size_t fsm = small_final_smem(pl.cap);
         if (smem_optin(gb_small_final_kernel, &c) != cudaSuccess)
             return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: shared-memory attribute failed");
-        gb_small_final_kernel<<<1, 1024, fsm, s>>>(d_final);
+        gb_small_final_kernel<<<1, SF_BLOCK, fsm, s>>>(d_final);
         if (cudaGetLastError() != cudaSuccess) return report(BOLT_ERR_CUDA, "bolt_groupby_noalloc: finalize launch failed");
         ull w[5] = {0, 0, 0, 0, 0};
         if (cudaMemcpyAsync(w, words, sizeof w, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -2130,7 +2245,8 @@ extern "C" bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* qs, int32_t
         ctx->last_error.clear();
         for (int i : idx)
             qs[i].status = gb_single(ctx, &qs[i].desc, &qs[i].out, qs[i].row_begin, qs[i].row_end,
-                                     flags & ~BOLT_FLAG_PROFILE, s, nullptr, nullptr, "batched GROUP BY");
+                                     flags & ~(BOLT_FLAG_PROFILE | BOLT_FLAG_KERNEL_TIMES), s, nullptr, nullptr,
+                                     "batched GROUP BY");
         for (int i = 0; i < n; ++i)
             if (qs[i].status != BOLT_OK)
                 return fail(ctx, qs[i].status, "batched GROUP BY: query %d failed (%s)", i,
@@ -2169,8 +2285,9 @@ extern "C" bolt_status bolt_batch_groupby(bolt_ctx* ctx, bolt_query* qs, int32_t
     }
     for (int i : redo) {
         bolt_query& q = qs[i];
-        q.status = gb_single(ctx, &q.desc, &q.out, q.row_begin, q.row_end, flags & ~BOLT_FLAG_PROFILE, s, nullptr,
-                             nullptr, "batched GROUP BY");
+        q.status = gb_single(ctx, &q.desc, &q.out, q.row_begin, q.row_end,
+                             flags & ~(BOLT_FLAG_PROFILE | BOLT_FLAG_KERNEL_TIMES), s, nullptr, nullptr,
+                             "batched GROUP BY");
     }
     ctx->last_error.clear();
     for (int i = 0; i < n; ++i)

@@ -857,7 +857,7 @@ void pred_range(int cmp, ll lit, int32_t& lo, int32_t& hi, int32_t& neg) {
 bool gb_lean_applies(const GbPlan& pl, uint32_t flags) {
     const GbParams& p = pl.prm;
     if (flags & (BOLT_FLAG_FORCE_GLOBAL | BOLT_FLAG_FORCE_SHMEM | BOLT_FLAG_KERNEL_REGS)) return false;
-    if (p.jslots || p.spec == 0 || p.spec == 3 || p.n_rows < (1ull << 22) || p.n_rows >= (1ull << 31)) return false;
+    if (p.jslots || p.spec == 0 || p.spec == 3 || p.n_rows < GB_LEAN_MIN_ROWS || p.n_rows >= (1ull << 31)) return false;
     // Dense columns only; 32-bit integer keys (one or two) or one 64-bit
     // integer key; at most one WHERE conjunct, on a 32-bit integer column;
     // at most GB_PART_MAX_FIELDS distinct value columns.

@@ -12,6 +12,8 @@ constexpr int GB_KP_I64 = 2;    // one Int64 key column
 
 constexpr int GB_PART_MAX_FIELDS = 3;                // distinct value columns a spilled row carries
 constexpr uint64_t GB_PART_MIN_GROUPS = 1ull << 15;  // expected groups from which the tier is used
+constexpr uint64_t GB_LEAN_MIN_ROWS = 1ull << 18;    // rows from which the streaming kernel serves a query
+constexpr uint64_t GB_STAGED_MIN_ROWS = 1ull << 22;  // rows from which the generic staged kernel is used untuned
 constexpr uint64_t GB_PART_RED_GROUPS = 512;         // expected groups per partition
 constexpr int GB_PART_MAX_PBITS = 13;                // at most 8192 partitions
 

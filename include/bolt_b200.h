@@ -97,6 +97,8 @@ typedef struct bolt_ctx bolt_ctx;
 #define BOLT_FLAG_NO_PART      0x80u /* GROUP BY: never use the hash-partitioned tier (global hash table instead) */
 #define BOLT_FLAG_FORCE_PART   0x100u /* GROUP BY: use the hash-partitioned tier wherever it applies, whatever the
                                         groups hint (testing) */
+#define BOLT_FLAG_KERNEL_TIMES 0x200u /* record only the dominant kernel's device time (bolt_ctx_kernel_times), not
+                                        the whole call's: two events per call instead of four */
 
 /* ------------------------------------------------------------------------ */
 /* Context: device, scratch arena, tuning cache, status word, last error.   */
@@ -119,7 +121,7 @@ uint32_t    bolt_ctx_last_launches(const bolt_ctx* ctx);
  * (the reference's Tier-1 / Tier-2 executors); 0 before any GROUP BY. */
 int32_t     bolt_ctx_last_groupby_tier(const bolt_ctx* ctx);
 /* Device milliseconds of the dominant kernel of every call made with
- * BOLT_FLAG_PROFILE since the previous read (up to 256 calls, oldest first).
+ * BOLT_FLAG_PROFILE or BOLT_FLAG_KERNEL_TIMES since the previous read (up to 256 calls, oldest first).
  * Waits for those kernels; returns how many times were written to `ms`. */
 uint32_t    bolt_ctx_kernel_times(bolt_ctx* ctx, double* ms, uint32_t max);
 /* Waits for the stream and returns the device-recorded status of every
