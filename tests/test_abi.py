@@ -105,3 +105,31 @@ def test_footprint_tracks_rows_not_only_the_hint(lib):
     assert small < big / 50
     sizes = [lib.bolt_groupby_footprint(C.byref(d), n) for n in (1, 100, 10_000, 1_000_000, 10_000_000)]
     assert sizes == sorted(sizes)
+
+
+RUST_SYS = REPO / "rust" / "bolt_b200_sys.rs"
+
+
+def header_constants() -> dict[str, int]:
+    """Enum values and #define flags of the header, by name."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    vals = {m[0]: int(m[1], 0) for m in re.findall(r"#define\s+(BOLT_FLAG_[A-Z_]+)\s+(0x[0-9a-fA-F]+)u", text)}
+    for body in re.findall(r"typedef enum\s*\{(.*?)\}", text, flags=re.S):
+        for name, val in re.findall(r"(BOLT_[A-Z0-9_]+)\s*=\s*(\d+)", body):
+            vals[name] = int(val)
+    return vals
+
+
+def test_rust_ffi_declares_every_function_and_constant():
+    """The Rust FFI file a maintainer drops into the reference declares every
+    entry point of the header and carries the header's constant values (it
+    is not compiled here: there is no Rust toolchain)."""
+    rs = RUST_SYS.read_text()
+    declared = set(re.findall(r"pub fn (bolt_[a-z0-9_]+)\s*\(", rs))
+    missing = [n for n in header_functions() if n not in declared]
+    assert not missing, f"rust/bolt_b200_sys.rs lacks {missing}"
+    consts = {m[0]: int(m[1], 0) for m in re.findall(r"pub const (BOLT_[A-Z0-9_]+): [a-z0-9_]+ = (0x[0-9a-fA-F]+|\d+);", rs)}
+    want = header_constants()
+    assert len(want) >= 30
+    wrong = {k: (consts.get(k), v) for k, v in want.items() if consts.get(k) != v}
+    assert not wrong, f"rust constants differ from the header (rust, header): {wrong}"
