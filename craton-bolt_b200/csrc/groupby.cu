@@ -418,10 +418,6 @@ __global__ void __launch_bounds__(1024, 1) gb_staged_kernel(const __grid_constan
 // ---------------------------------------------------------------------------
 // Finalize
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void write_bit(uint8_t* bm, uint64_t i, bool on) {
-    if (bm) set_bit_atomic(bm, i, on);
-}
-
 __device__ __forceinline__ double sum_as_double(const GbFinal& f, const StateDesc& s, const ull* w) {
     switch (s.kind) {
     case K_SUM_I32: return (double)(ll)w[0];
@@ -439,8 +435,11 @@ __device__ __forceinline__ double sum_as_double(const GbFinal& f, const StateDes
     }
 }
 
-// Writes output row o from slot `slot` (slot == cap + 1 is the NULL group).
-__device__ void emit_group(const GbFinal& f, uint64_t o, uint64_t slot) {
+// Writes output row o from slot `slot` (slot == cap + 1 is the NULL group)
+// and returns its validity bits: bit k for key column k, bit n_keys + a for
+// aggregate column a (write_valid_words stores them).
+__device__ __forceinline__ uint32_t emit_group(const GbFinal& f, uint64_t o, uint64_t slot) {
+    uint32_t vbits = 0;
     const ull cap = 1ull << f.log2cap;
     const ull* w = f.gtab + slot * (ull)f.slot_words;
     const bool null_key = slot == cap + 1;
@@ -454,7 +453,7 @@ __device__ void emit_group(const GbFinal& f, uint64_t o, uint64_t slot) {
         case BOLT_F32: ((uint32_t*)out)[o] = (uint32_t)bits; break;
         default: ((ull*)out)[o] = bits; break;
         }
-        write_bit(f.out_key_valid[k], o, !null_key);
+        if (!null_key) vbits |= 1u << k;
     }
     for (int a = 0; a < f.n_aggs; ++a) {
         const AggOut& g = f.agg[a];
@@ -506,7 +505,27 @@ __device__ void emit_group(const GbFinal& f, uint64_t o, uint64_t slot) {
             }
         }
         }
-        write_bit(g.out_valid, o, valid);
+        if (valid) vbits |= 1u << (f.n_keys + a);
+    }
+    return vbits;
+}
+
+// Validity bitmaps of output rows [o0, o0 + 32) from one warp (o0 a multiple
+// of 32, lanes past the rows pass row = false): one ballot per column and
+// byte stores by lane 0, so no two warps share a byte and no atomics are
+// needed; bytes past the last output row are not written.
+__device__ __forceinline__ void write_valid_words(const GbFinal& f, uint64_t o0, uint64_t lim, uint32_t vbits,
+                                                  bool row) {
+    const uint64_t nbytes = (lim + 7) / 8;
+    const int nc = f.n_keys + f.n_aggs;
+    for (int c = 0; c < nc; ++c) {
+        uint8_t* bm = c < f.n_keys ? f.out_key_valid[c] : f.agg[c - f.n_keys].out_valid;
+        const uint32_t m = __ballot_sync(0xffffffffu, row && ((vbits >> c) & 1u));
+        if (bm && lane_id() == 0) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (o0 / 8 + b < nbytes) bm[o0 / 8 + b] = (uint8_t)(m >> (8 * b));
+        }
     }
 }
 
@@ -612,13 +631,21 @@ __global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fin
         }
         const ull lim = total < f.out_cap ? total : f.out_cap;
         const uint64_t c1 = c0 + FIN_CHUNK < lim ? c0 + FIN_CHUNK : lim;
-        for (uint64_t o = c0 + threadIdx.x; o < c1; o += blockDim.x) {
-            const uint64_t slot = o < G ? f.sorted[o] : cap + 1;
-            if (slot > cap + 1) {  // (a sort entry nobody wrote: never read past the table)
-                atomicOr(f.status, ST_FLAG_INTERNAL);
-                continue;
+        // Warp-uniform rows of 32 (c0 and blockDim are multiples of 32).
+        for (uint64_t o0 = c0 + (threadIdx.x & ~31u); o0 < c1; o0 += blockDim.x) {
+            const uint64_t o = o0 + lane_id();
+            bool row = o < c1;
+            uint32_t vb = 0;
+            if (row) {
+                const uint64_t slot = o < G ? f.sorted[o] : cap + 1;
+                if (slot > cap + 1) {  // (a sort entry nobody wrote: never read past the table)
+                    atomicOr(f.status, ST_FLAG_INTERNAL);
+                    row = false;
+                } else {
+                    vb = emit_group(f, o, slot);
+                }
             }
-            emit_group(f, o, slot);
+            write_valid_words(f, o0, lim, vb, row);
         }
     }
 }
@@ -776,7 +803,12 @@ __device__ __forceinline__ void small_final_body(const GbFinal& f) {
         if (total > f.out_cap) atomicOr(f.status, ST_FLAG_CAPACITY);
     }
     const ull lim = total < f.out_cap ? total : f.out_cap;
-    for (uint64_t o = threadIdx.x; o < lim; o += blockDim.x) emit_group(f, o, o < G ? sorted[o] : cap + 1);
+    for (uint64_t o0 = threadIdx.x & ~31u; o0 < lim; o0 += blockDim.x) {  // (warp-uniform)
+        const uint64_t o = o0 + lane;
+        const bool row = o < lim;
+        const uint32_t vb = row ? emit_group(f, o, o < G ? sorted[o] : cap + 1) : 0u;
+        write_valid_words(f, o0, lim, vb, row);
+    }
 }
 
 // Several queries, one CTA each (descriptors in device memory).

@@ -150,3 +150,28 @@ def test_join_groupby_extreme_keys_and_nulls(bolt, engine, oracle, kdt):
     amt = np.stack([rng.integers(-10**6, 10**6, npr), np.zeros(npr, np.int64)], axis=1).astype(np.int64)
     amt[:, 1] = amt[:, 0] >> 63
     _join_groupby_vs_oracle(bolt, engine, oracle, bk, bg, pk, amt, kdt, bvalid, pvalid)
+
+
+@pytest.mark.parametrize("kdt", ["i32", "i64"])
+def test_join_groupby_table_larger_than_l2(bolt, engine, oracle, kdt):
+    """A 3M-key build side (8M slots, 128 MB table, larger than L2) probed by
+    12M rows: keys -1, 0 and the dtype's extremes, 10 % absent probe keys;
+    equals the oracle exactly."""
+    rng = np.random.default_rng(23)
+    nb, npr = 3_000_000, 12_000_000
+    info = np.iinfo(np.int32 if kdt == "i32" else np.int64)
+    special = np.array([-1, 0, info.min, info.max], dtype=np.int64)
+    if kdt == "i32":  # an odd multiplier permutes [0, 2^31)
+        rest = (np.arange(1, nb + 1, dtype=np.int64) * 2654435761) % (2**31)
+    else:  # ... and [0, 2^64)
+        rest = (np.arange(1, nb + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)).view(np.int64)
+    rest = np.setdiff1d(rest, special)[: nb - len(special)]
+    bk = rng.permutation(np.concatenate([special, rest])).astype(np.int32 if kdt == "i32" else np.int64)
+    bg = rng.integers(0, 1000, len(bk)).astype(np.int32)
+    pk = bk[rng.integers(0, len(bk), npr)].copy()
+    absent = rng.random(npr) < 0.1
+    pk[absent] = -2  # never a build key (the build keys are -1, 0, extremes and non-negative values)
+    amt = np.stack([rng.integers(-10**9, 10**9, npr), np.zeros(npr, np.int64)], axis=1).astype(np.int64)
+    amt[:, 1] = amt[:, 0] >> 63
+    assert -2 not in set(special.tolist())
+    _join_groupby_vs_oracle(bolt, engine, oracle, bk, bg, pk, amt, kdt)
