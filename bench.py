@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import importlib
 import importlib.util
 import json
@@ -762,14 +763,22 @@ def w_batch(c: Ctx):
             prepared3 = [prep(q) for q in qs]
             torch.cuda.synchronize()
             tickets = []
-            t0 = time.perf_counter()
-            nxt = t0
-            for pq, gap in zip(prepared3, gaps):
-                nxt += gap
-                while time.perf_counter() < nxt:
-                    pass
-                tickets.append(srv.submit(pq))
-            lat_poisson = [srv.wait(t)[1] for t in tickets]
+            # No collector pause inside the arrival loop: a full collection over
+            # the prepared queries stalls the submitter for tens of
+            # milliseconds, which then submits the overdue arrivals at once.
+            gc.collect()
+            gc.disable()
+            try:
+                t0 = time.perf_counter()
+                nxt = t0
+                for pq, gap in zip(prepared3, gaps):
+                    nxt += gap
+                    while time.perf_counter() < nxt:
+                        pass
+                    tickets.append(srv.submit(pq))
+                lat_poisson = [srv.wait(t)[1] for t in tickets]
+            finally:
+                gc.enable()
         finally:
             srv.close()
         # The same Poisson arrivals served one query at a time (FIFO): latency
@@ -777,17 +786,22 @@ def w_batch(c: Ctx):
         prepared4 = [prep(q, sliced=True) for q in qs]
         torch.cuda.synchronize()
         lat_single_poisson = []
-        t0 = time.perf_counter()
-        arrive = t0
-        for pq, gap in zip(prepared4, gaps):
-            arrive += gap
-            while time.perf_counter() < arrive:
-                pass
-            st = c.lib.bolt_groupby(c.eng._ctx, C.byref(pq.desc), C.byref(pq.out), 0,
-                                    C.c_void_p(c.stream.cuda_stream))
-            if st != 0:
-                raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
-            lat_single_poisson.append((time.perf_counter() - arrive) * 1e6)
+        gc.collect()
+        gc.disable()
+        try:
+            t0 = time.perf_counter()
+            arrive = t0
+            for pq, gap in zip(prepared4, gaps):
+                arrive += gap
+                while time.perf_counter() < arrive:
+                    pass
+                st = c.lib.bolt_groupby(c.eng._ctx, C.byref(pq.desc), C.byref(pq.out), 0,
+                                        C.c_void_p(c.stream.cuda_stream))
+                if st != 0:
+                    raise RuntimeError(c.lib.bolt_ctx_last_error(c.eng._ctx).decode())
+                lat_single_poisson.append((time.perf_counter() - arrive) * 1e6)
+        finally:
+            gc.enable()
         del prepared4
         return {"queries": len(qs), "rows_total": total_rows, "batched_qps": batch_qps,
                 "one_at_a_time_qps": single_qps, "speedup": batch_qps / single_qps,
