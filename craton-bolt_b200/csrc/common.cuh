@@ -125,7 +125,9 @@ __device__ __forceinline__ double i128_to_double_scaled(ull lo, ll hi, int e) {
         if (rem > half || (rem == half && ((ull)mant & 1ull))) mant += 1;
         d = (double)(ull)mant;  // <= 2^53, exact
     }
-    d = scalbn(d, shift - e);
+    // d * 2^(shift - e) by one multiply with the exact power of two: the
+    // callers' scales (0 <= e <= 94, shift <= 75) keep it a normal double.
+    d *= __longlong_as_double((long long)(1023 + shift - e) << 52);
     return neg ? -d : d;
 }
 
