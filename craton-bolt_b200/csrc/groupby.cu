@@ -549,6 +549,9 @@ __device__ __forceinline__ int query_of(const uint32_t* begins, int nq, uint32_t
 }
 
 constexpr int FIN_CHUNK = 4096;
+// Output rows per gather work item (a multiple of 32: each warp owns whole
+// validity words); smaller than FIN_CHUNK so the rows spread over every CTA.
+constexpr int GATHER_CHUNK = 1024;
 
 // Occupied-slot compaction of the large-table queries: work items are
 // (query, chunk of 4096 slots); order key = packed key ^ sign bit.
@@ -611,7 +614,7 @@ __global__ void __launch_bounds__(256) gb_compact_batch_kernel(const GbFinal* fi
 }
 
 // Output rows of the large-table queries: work items are (query, chunk of
-// 4096 output rows) up to cap + 1 rows; rows past the group count exit.
+// GATHER_CHUNK output rows) up to cap + 1 rows; rows past the group count exit.
 __global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fins, const uint32_t* begins, int nq,
                                                                uint32_t total_items) {
     __shared__ __align__(16) GbFinal f;
@@ -623,14 +626,14 @@ __global__ void __launch_bounds__(256) gb_gather_batch_kernel(const GbFinal* fin
         const ull G = min(*f.n_nonnull, f.n_max);  // (a counter that ran past the table flagged GROW)
         const bool has_null = f.gtab[(cap + 1) * (ull)f.slot_words] != 0;
         const ull total = G + (has_null ? 1 : 0);
-        const uint64_t c0 = (uint64_t)(item - begins[q]) * FIN_CHUNK;
+        const uint64_t c0 = (uint64_t)(item - begins[q]) * GATHER_CHUNK;
         if (c0 == 0 && threadIdx.x == 0) {
             *f.n_groups = total;
             if (f.n_groups_user) *f.n_groups_user = total;
             if (total > f.out_cap) atomicOr(f.status, ST_FLAG_CAPACITY);
         }
         const ull lim = total < f.out_cap ? total : f.out_cap;
-        const uint64_t c1 = c0 + FIN_CHUNK < lim ? c0 + FIN_CHUNK : lim;
+        const uint64_t c1 = c0 + GATHER_CHUNK < lim ? c0 + GATHER_CHUNK : lim;
         // Warp-uniform rows of 32 (c0 and blockDim are multiples of 32).
         for (uint64_t o0 = c0 + (threadIdx.x & ~31u); o0 < c1; o0 += blockDim.x) {
             const uint64_t o = o0 + lane_id();
@@ -1588,7 +1591,7 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
     if (!large_q.empty()) {
         const int nl = (int)large_q.size();
         std::vector<uint32_t> cbeg(nl + 1), gbeg(nl + 1);
-        uint64_t citems = 0;
+        uint64_t citems = 0, gitems = 0;
         SortSpec sp;
         sp.src = SRC_U64_KEYS;
         for (int i = 0; i < nl; ++i) {
@@ -1605,6 +1608,8 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
             large.push_back(f);
             cbeg[i] = (uint32_t)citems;
             citems += (g + FIN_CHUNK - 1) / FIN_CHUNK;
+            gbeg[i] = (uint32_t)gitems;
+            gitems += (g + GATHER_CHUNK - 1) / GATHER_CHUNK;
             SortSegment seg;
             seg.keys = f.order_keys;
             seg.payload_in = f.slots;
@@ -1614,11 +1619,15 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
             sp.segs.push_back(seg);
         }
         cbeg[nl] = (uint32_t)citems;
+        gbeg[nl] = (uint32_t)gitems;
         GbFinal* d_f = (GbFinal*)arena_alloc(ctx, sizeof(GbFinal) * nl);
         uint32_t* d_beg = (uint32_t*)arena_alloc(ctx, 4ull * (nl + 1));
-        if (!d_f || !d_beg) return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
+        uint32_t* d_gbeg = (uint32_t*)arena_alloc(ctx, 4ull * (nl + 1));
+        if (!d_f || !d_beg || !d_gbeg)
+            return fail(ctx, BOLT_ERR_CAPACITY, "GROUP BY: scratch arena too small for the finalize");
         bolt_status st = stage_upload(ctx, s, d_f, large.data(), sizeof(GbFinal) * nl);
         if (st == BOLT_OK) st = stage_upload(ctx, s, d_beg, cbeg.data(), 4ull * (nl + 1));
+        if (st == BOLT_OK) st = stage_upload(ctx, s, d_gbeg, gbeg.data(), 4ull * (nl + 1));
         if (st != BOLT_OK) return st;
         const unsigned cg = (unsigned)std::min<uint64_t>(citems, (uint64_t)ctx->num_sms * 8);
         if (!pls[large_q[0]]->precompacted) {  // (a precompacted query is finalized alone)
@@ -1627,7 +1636,8 @@ static bolt_status gb_run_finalize(bolt_ctx* ctx, GbPlan** pls, int nq, cudaStre
         }
         st = radix_sort(ctx, s, sp);
         if (st != BOLT_OK) return st;
-        gb_gather_batch_kernel<<<cg, 256, 0, s>>>(d_f, d_beg, nl, (uint32_t)citems);
+        const unsigned gg = (unsigned)std::min<uint64_t>(gitems, (uint64_t)ctx->num_sms * 8);
+        gb_gather_batch_kernel<<<gg, 256, 0, s>>>(d_f, d_gbeg, nl, (uint32_t)gitems);
         ctx->last_launches++;
     }
     BOLT_CUDA(ctx, cudaGetLastError());
