@@ -407,8 +407,12 @@ class Engine:
     def hash_join_indices(self, build_key: Column, probe_key: Column, out_cap: int | None = None,
                           flags: int = 0):
         """INNER equi-join: (probe_idx, build_idx) u32 pairs in probe order
-        (hash_join_indices_on_gpu, src/exec/gpu_join.rs:1403). Returns None on
-        a decline (duplicate build keys, unsupported dtype)."""
+        (hash_join_indices_on_gpu, src/exec/gpu_join.rs:1403); a build key
+        that occurs several times pairs with each of its build rows in
+        ascending row order (the reference's host join, src/exec/join.rs:
+        407-425). Returns None on a decline (unsupported dtype). Without
+        `out_cap` the output is sized to the probe rows and, when duplicate
+        build keys produce more pairs, to the count the probe reports."""
         bk, pk = self._dev(build_key), self._dev(probe_key)
         table = C.c_void_p()
         st = self._lib.bolt_hash_join_build(self._ctx, C.byref(bk.view()), None, flags | FLAG_PROFILE,
@@ -417,14 +421,19 @@ class Engine:
             return None
         try:
             cap = len(pk) if out_cap is None else out_cap
-            pi = torch.empty(max(cap, 1), dtype=torch.int32, device=f"cuda:{self.device}")
-            bi = torch.empty(max(cap, 1), dtype=torch.int32, device=f"cuda:{self.device}")
-            n_out = C.c_uint64(0)
-            st = self._lib.bolt_hash_join_probe(self._ctx, table, C.byref(pk.view()),
-                                                C.byref(_abi.ColMut(pi.data_ptr(), None, cap, _abi.U32, 0)),
-                                                C.byref(_abi.ColMut(bi.data_ptr(), None, cap, _abi.U32, 0)),
-                                                C.byref(n_out), flags | FLAG_PROFILE,
-                                                C.c_void_p(self.stream_handle))
+            for _attempt in range(2):
+                pi = torch.empty(max(cap, 1), dtype=torch.int32, device=f"cuda:{self.device}")
+                bi = torch.empty(max(cap, 1), dtype=torch.int32, device=f"cuda:{self.device}")
+                n_out = C.c_uint64(0)
+                st = self._lib.bolt_hash_join_probe(self._ctx, table, C.byref(pk.view()),
+                                                    C.byref(_abi.ColMut(pi.data_ptr(), None, cap, _abi.U32, 0)),
+                                                    C.byref(_abi.ColMut(bi.data_ptr(), None, cap, _abi.U32, 0)),
+                                                    C.byref(n_out), flags | FLAG_PROFILE,
+                                                    C.c_void_p(self.stream_handle))
+                if st == _abi.ERR_CAPACITY and out_cap is None and int(n_out.value) > cap:
+                    cap = int(n_out.value)
+                    continue
+                break
             self._check(st, "hash join probe")
             k = int(n_out.value)
             return pi[:k], bi[:k]
@@ -435,7 +444,8 @@ class Engine:
                      max_groups: int = 1 << 16, flags: int = 0):
         """SELECT b.g, SUM(p.value), COUNT(*) FROM p JOIN b ON p.key = b.key
         GROUP BY b.g, without materialising the join. Returns
-        (group Column, sum Column, count Column) sorted by group."""
+        (group Column, sum Column, count Column) sorted by group, or None on a
+        decline (duplicate build keys: join with hash_join_indices instead)."""
         bk, bg, pk, val = self._dev(build_key), self._dev(build_group), self._dev(probe_key), self._dev(value)
         table = C.c_void_p()
         st = self._lib.bolt_hash_join_build(self._ctx, C.byref(bk.view()), C.byref(bg.view()),
@@ -453,7 +463,8 @@ class Engine:
                                              C.byref(self._mut(g, max_groups)), C.byref(self._mut(s, max_groups)),
                                              C.byref(self._mut(c, max_groups)), C.byref(n_out),
                                              flags | FLAG_PROFILE, C.c_void_p(self.stream_handle))
-            self._check(st, "join GROUP BY")
+            if not self._check(st, "join GROUP BY", decline_ok=True):
+                return None
             k = int(n_out.value)
             return self._trim(g, k), self._trim(s, k), self._trim(c, k)
         finally:

@@ -2227,6 +2227,8 @@ extern "C" bolt_status bolt_join_groupby(bolt_ctx* ctx, const bolt_join_table* t
     if (!t || !probe_key || !value || !out_group || !out_sum || !out_count || !n_groups)
         return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: bad arguments");
     if (!t->has_payload) return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: the table was built without a payload");
+    if (t->multi)  // one aggregation row per probe row: a key with several build rows does not fit
+        return fail(ctx, BOLT_DECLINE, "join GROUP BY: duplicate build keys");
     if (probe_key->dtype != BOLT_I32 && probe_key->dtype != BOLT_I64)
         return fail(ctx, BOLT_DECLINE, "join GROUP BY: probe key dtype %d", probe_key->dtype);
     if (value->len != probe_key->len) return fail(ctx, BOLT_ERR_INVALID, "join GROUP BY: column lengths differ");

@@ -16,6 +16,9 @@
 
 #include <algorithm>
 
+#include "compact.cuh"
+#include "radix_sort.cuh"
+
 namespace bolt {
 namespace {
 
@@ -84,11 +87,16 @@ struct ProbeArgs {
     uint32_t* tile_ctr;
     ull* n_out;
     uint32_t* status;
+    const uint32_t* sorted_rows;  // multi-match tables only
 };
 
+// MULTI: the table maps a key to a run of sorted_rows (duplicate build keys):
+// a probe row emits one pair per build row of its run, in build-row order, at
+// a position from the tile's prefix of match counts.
+template <bool MULTI>
 __global__ void __launch_bounds__(JP_BLOCK) join_probe_kernel(const __grid_constant__ ProbeArgs a) {
     __shared__ uint32_t s_tile;
-    __shared__ uint32_t cnt[JP_ITEMS][JP_NW];
+    __shared__ ull cnt[JP_ITEMS][JP_NW];
     __shared__ ull s_base;
     const uint32_t ntiles = (uint32_t)((a.n + JP_TILE - 1) / JP_TILE);
     if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
@@ -97,7 +105,9 @@ __global__ void __launch_bounds__(JP_BLOCK) join_probe_kernel(const __grid_const
     if (tile >= ntiles) return;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t base = (uint64_t)tile * JP_TILE;
-    uint32_t brow[JP_ITEMS];
+    uint32_t brow[JP_ITEMS];  // build row, or (MULTI) first position of the run
+    uint32_t nm[JP_ITEMS];    // (MULTI) build rows matched
+    ull wex[JP_ITEMS];        // (MULTI) matches of the warp's earlier lanes
     uint32_t hit = 0;
 #pragma unroll
     for (int j = 0; j < JP_ITEMS; ++j) {
@@ -105,30 +115,45 @@ __global__ void __launch_bounds__(JP_BLOCK) join_probe_kernel(const __grid_const
         ull k;
         bool m = false;
         brow[j] = 0;
+        nm[j] = 0;
+        wex[j] = 0;
         if (e < a.n && load_join_key(a.key, a.kdt, a.kvalid, e, k)) {
             const ull w1 = join_lookup(a.slots, a.log2cap, k);
             if (w1 != ~0ull) {
                 m = true;
                 brow[j] = (uint32_t)(w1 >> 32);
+                nm[j] = MULTI ? (uint32_t)w1 : 1u;
             }
         }
-        const uint32_t b = __ballot_sync(0xffffffffu, m);
-        if (lane == 0) cnt[j][w] = __popc(b);
+        if (MULTI) {
+            ull x = nm[j];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const ull y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            wex[j] = x - nm[j];
+            const ull tot = __shfl_sync(0xffffffffu, x, 31);
+            if (lane == 0) cnt[j][w] = tot;
+        } else {
+            const uint32_t b = __ballot_sync(0xffffffffu, m);
+            if (lane == 0) cnt[j][w] = __popc(b);
+        }
         if (m) hit |= 1u << j;
     }
     __syncthreads();
     if (w == 0) {
-        uint32_t local = 0;
+        ull local = 0;
 #pragma unroll
         for (int j = 0; j < JP_ITEMS; ++j) {
-            const uint32_t v = lane < JP_NW ? cnt[j][lane] : 0;
-            uint32_t x = v;
+            const ull v = lane < JP_NW ? cnt[j][lane] : 0ull;
+            ull x = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                const ull y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += y;
             }
-            const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+            const ull tot = __shfl_sync(0xffffffffu, x, 31);
             if (lane < JP_NW) cnt[j][lane] = local + x - v;
             local += tot;
         }
@@ -170,6 +195,14 @@ __global__ void __launch_bounds__(JP_BLOCK) join_probe_kernel(const __grid_const
 #pragma unroll
     for (int j = 0; j < JP_ITEMS; ++j) {
         const uint64_t e = base + (uint64_t)j * JP_BLOCK + threadIdx.x;
+        if (MULTI) {
+            const ull pos = tbase + cnt[j][w] + wex[j];
+            for (uint32_t t = 0; t < nm[j] && pos + t < a.out_cap; ++t) {
+                a.out_probe[pos + t] = (uint32_t)e;
+                a.out_build[pos + t] = a.sorted_rows[(uint64_t)brow[j] + t];
+            }
+            continue;
+        }
         const uint32_t b = __ballot_sync(0xffffffffu, (hit >> j) & 1u);
         if (!((hit >> j) & 1u)) continue;
         const ull pos = tbase + cnt[j][w] + __popc(b & lanemask_lt());
@@ -177,6 +210,123 @@ __global__ void __launch_bounds__(JP_BLOCK) join_probe_kernel(const __grid_const
         a.out_probe[pos] = (uint32_t)e;
         a.out_build[pos] = brow[j];
     }
+}
+
+// Multi-match build, step 1: flag[i] = 1 where sorted position i starts a run
+// of equal keys (the rows are the non-NULL build rows stably sorted by key).
+__global__ void __launch_bounds__(256) jm_mark_kernel(const void* key, int kdt, const uint32_t* sorted, uint64_t nv,
+                                                       uint8_t* flag) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x) {
+        const ull k = kdt == BOLT_I32 ? (ull)(ll)__ldg((const int32_t*)key + sorted[i]) : (ull)__ldg((const ll*)key + sorted[i]);
+        bool start = i == 0;
+        if (!start) {
+            const ull kp = kdt == BOLT_I32 ? (ull)(ll)__ldg((const int32_t*)key + sorted[i - 1])
+                                           : (ull)__ldg((const ll*)key + sorted[i - 1]);
+            start = k != kp;
+        }
+        flag[i] = start ? 1 : 0;
+    }
+}
+
+// Multi-match build, step 2: one table entry per run: word 1 = (first sorted
+// position << 32) | run length. The keys are distinct now, so a CAS that
+// finds the key already present cannot happen.
+__global__ void __launch_bounds__(256) jm_insert_kernel(ull* slots, int log2cap, const void* key, int kdt,
+                                                         const uint32_t* sorted, const uint32_t* starts, uint64_t nruns,
+                                                         uint64_t nv, uint32_t* status) {
+    const ull cap = 1ull << log2cap;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nruns; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t start = starts[r];
+        const uint64_t end = r + 1 < nruns ? starts[r + 1] : nv;
+        const uint32_t row = sorted[start];
+        const ull k = kdt == BOLT_I32 ? (ull)(ll)__ldg((const int32_t*)key + row) : (ull)__ldg((const ll*)key + row);
+        const ull stored = ~k;
+        const ull w1 = ((ull)start << 32) | (ull)(end - start);
+        if (stored == 0) {
+            ull* sp = slots + 2 * cap;
+            sp[1] = w1;
+            sp[0] = 1ull;
+            continue;
+        }
+        ull h = (stored * JOIN_HASH) >> (64 - log2cap);
+        bool placed = false;
+        for (ull t = 0; t < cap; ++t) {
+            ull* sp = slots + 2 * h;
+            if (atomicCAS(sp, 0ull, stored) == 0) {
+                sp[1] = w1;
+                placed = true;
+                break;
+            }
+            h = (h + 1) & (cap - 1);
+        }
+        if (!placed) atomicOr(status, ST_FLAG_SPILL);
+    }
+}
+
+// Rebuilds table t as a multi-match table (the unique-key build found a
+// duplicate key): the non-NULL build rows are stably sorted by key (so each
+// key's rows stay in ascending order, as in the reference's host join map,
+// src/exec/join.rs:843-855), runs of equal keys are marked and compacted, and
+// each key maps to its run. The sorted rows stay pinned above the table.
+bolt_status join_build_multi(bolt_ctx* ctx, cudaStream_t s, bolt_join_table* t, const bolt_col_view* bk) {
+    const uint64_t n = bk->len;
+    const uint64_t bytes = ((1ull << t->log2cap) + 1) * 16;
+    ctx->arena_used = ctx->arena_pinned;
+    uint32_t* sorted = (uint32_t*)arena_alloc(ctx, (n ? n : 1) * 4);
+    if (!sorted) return fail(ctx, BOLT_ERR_CAPACITY, "hash join build: no room for the sorted build rows");
+    ctx->arena_pinned = ctx->arena_used;
+    ull* cnt = (ull*)arena_alloc(ctx, 64);
+    uint32_t* valid_ids = bk->validity ? (uint32_t*)arena_alloc(ctx, (n ? n : 1) * 4) : nullptr;
+    uint8_t* flag = (uint8_t*)arena_alloc(ctx, n ? n : 1);
+    uint32_t* starts = (uint32_t*)arena_alloc(ctx, (n ? n : 1) * 4);
+    if (!cnt || !flag || !starts || (bk->validity && !valid_ids))
+        return fail(ctx, BOLT_ERR_CAPACITY, "hash join build: scratch arena too small for duplicate keys");
+    BOLT_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 16, s));
+    BOLT_CUDA(ctx, cudaMemsetAsync(t->slots, 0, bytes, s));
+    uint64_t nv = n;
+    if (bk->validity) {  // NULL keys never match: sort only the valid rows
+        CompactSpec cv;
+        cv.n = n;
+        cv.keep_valid_of = bk->validity;
+        cv.row_ids = valid_ids;
+        cv.n_out_dev = cnt;
+        bolt_status st = compact_enqueue(ctx, s, cv);
+        if (st != BOLT_OK) return st;
+        BOLT_CUDA(ctx, cudaMemcpyAsync(ctx->h_words, cnt, 8, cudaMemcpyDeviceToHost, s));
+        BOLT_CUDA(ctx, cudaStreamSynchronize(s));
+        nv = ctx->h_words[0];
+    }
+    t->multi = 1;
+    t->sorted_rows = sorted;
+    if (nv == 0) return BOLT_OK;
+    SortSpec sp;
+    sp.src = bk->dtype == BOLT_I32 ? SRC_I32 : SRC_I64;
+    sp.indirect = valid_ids ? 1 : 0;
+    SortSegment seg;
+    seg.keys = bk->data;
+    seg.payload_in = valid_ids;
+    seg.payload_out = sorted;
+    seg.n = nv;
+    sp.segs.push_back(seg);
+    bolt_status st = radix_sort(ctx, s, sp);
+    if (st != BOLT_OK) return st;
+    const unsigned g = grid_for(nv, 256, ctx->num_sms * 16);
+    jm_mark_kernel<<<g, 256, 0, s>>>(bk->data, bk->dtype, sorted, nv, flag);
+    CompactSpec cr;
+    cr.n = nv;
+    cr.mask = flag;
+    cr.row_ids = starts;
+    cr.n_out_dev = cnt;
+    st = compact_enqueue(ctx, s, cr);
+    if (st != BOLT_OK) return st;
+    BOLT_CUDA(ctx, cudaMemcpyAsync(ctx->h_words, cnt, 8, cudaMemcpyDeviceToHost, s));
+    BOLT_CUDA(ctx, cudaStreamSynchronize(s));
+    const uint64_t nruns = ctx->h_words[0];
+    jm_insert_kernel<<<grid_for(nruns, 256, ctx->num_sms * 16), 256, 0, s>>>(
+        t->slots, t->log2cap, bk->data, bk->dtype, sorted, starts, nruns, nv, ctx->d_status);
+    BOLT_CUDA(ctx, cudaGetLastError());
+    ctx->last_launches += 2;
+    return BOLT_OK;
 }
 
 }  // namespace
@@ -228,6 +378,11 @@ extern "C" bolt_status bolt_hash_join_build(bolt_ctx* ctx, const bolt_col_view* 
     if (!(flags & BOLT_FLAG_ASYNC)) {
         uint32_t f = 0;
         st = read_status(ctx, s, 0, &f);
+        if (st == BOLT_OK && f == ST_FLAG_DUPKEY) {
+            // Duplicate build keys: rebuild as a multi-match table.
+            st = join_build_multi(ctx, s, t, build_key);
+            if (st == BOLT_OK) st = read_status(ctx, s, 0, &f);
+        }
         if (st == BOLT_OK) st = flags_to_status(ctx, f, "hash join build");
         if (st != BOLT_OK) {
             ctx->arena_pinned = 0;
@@ -272,6 +427,7 @@ extern "C" bolt_status bolt_hash_join_probe(bolt_ctx* ctx, const bolt_join_table
     a.out_probe = (uint32_t*)probe_idx->data;
     a.out_build = (uint32_t*)build_idx->data;
     a.out_cap = std::min(probe_idx->cap, build_idx->cap);
+    a.sorted_rows = t->sorted_rows;
     const uint64_t ntiles = (a.n + JP_TILE - 1) / JP_TILE;
     a.lookback = (ull*)arena_alloc(ctx, (ntiles + 1) * 8);
     a.tile_ctr = (uint32_t*)arena_alloc(ctx, 64);
@@ -283,7 +439,8 @@ extern "C" bolt_status bolt_hash_join_probe(bolt_ctx* ctx, const bolt_join_table
     BOLT_CUDA(ctx, cudaMemsetAsync(a.n_out, 0, 64, s));
     if (ntiles) {
         kernel_mark_begin(ctx, flags, s);
-        join_probe_kernel<<<(unsigned)ntiles, JP_BLOCK, 0, s>>>(a);
+        if (t->multi) join_probe_kernel<true><<<(unsigned)ntiles, JP_BLOCK, 0, s>>>(a);
+        else join_probe_kernel<false><<<(unsigned)ntiles, JP_BLOCK, 0, s>>>(a);
         kernel_mark_end(ctx, flags, s);
         ctx->last_launches = 1;
     }

@@ -5,12 +5,16 @@
 
 // A build-side hash table in the context arena. Slot i holds two words:
 //   word 0: bitwise NOT of the key (0 = empty; key -1 lives in slot `cap`),
-//   word 1: (build row << 32) | u32 payload.
+//   word 1: (build row << 32) | u32 payload — or, in a multi-match table
+//           (duplicate build keys), (first position in sorted_rows << 32) |
+//           number of build rows with the key.
 struct bolt_join_table {
     ull* slots = nullptr;
     int32_t log2cap = 0;
     int32_t key_dtype = BOLT_I64;
     int32_t has_payload = 0;
+    int32_t multi = 0;                 // 1: duplicate build keys, word 1 as above
+    uint32_t* sorted_rows = nullptr;   // multi: the non-NULL build rows, stably sorted by key
     uint64_t n_build = 0;
     uint64_t pinned_mark = 0;  // arena_pinned before this table was placed
     bolt_ctx* owner = nullptr;

@@ -264,9 +264,14 @@ bolt_status bolt_ctx_tuning_load(bolt_ctx* ctx, const char* path);
 /* ------------------------------------------------------------------------ */
 typedef struct bolt_join_table bolt_join_table;
 
-/* Build: a duplicate build key returns BOLT_DECLINE (the reference routes
- * duplicate build keys to its collision-list path). `payload` (nullable) is
- * an I32 build column carried in the table for bolt_join_groupby. */
+/* Build. Duplicate build keys (the reference's collision-list path,
+ * src/jit/hash_join_kernel.rs:1183,1368) make a multi-match table: the
+ * probe then pairs each probe row with every build row of its key, in
+ * ascending build-row order (the reference's host join, src/exec/join.rs:
+ * 407-425, 843-855). With BOLT_FLAG_ASYNC the duplicate is only reported
+ * (BOLT_DECLINE at the status check) instead of rebuilt. `payload`
+ * (nullable) is an I32 build column carried in the table for
+ * bolt_join_groupby, which declines on a multi-match table. */
 bolt_status bolt_hash_join_build(bolt_ctx* ctx, const bolt_col_view* build_key,
                                  const bolt_col_view* payload, uint32_t flags,
                                  bolt_stream stream, bolt_join_table** table_out);

@@ -165,6 +165,27 @@ def hash_join(build_key: HostCol, probe_key: HostCol):
     return op[:k], ob[:k]
 
 
+def hash_join_multi(build_key: HostCol, probe_key: HostCol, cap: int | None = None):
+    """INNER join with any build keys (duplicates included): (probe_row,
+    build_row) pairs in probe order, then build-row order."""
+    nb, npr = len(build_key.data), len(probe_key.data)
+    if cap is None:
+        cap = max(npr, 1) * 4
+    op = np.zeros(max(cap, 1), np.uint32)
+    ob = np.zeros(max(cap, 1), np.uint32)
+    n = C.c_uint64(0)
+    f = lib().orc_hash_join_multi
+    f.restype = C.c_int
+    st = f(C.c_uint64(nb), C.byref(build_key.c()), C.c_uint64(npr), C.byref(probe_key.c()),
+           _ptr(op), _ptr(ob), C.c_uint64(cap), C.byref(n))
+    if st == CAPACITY:
+        return hash_join_multi(build_key, probe_key, int(n.value))
+    if st != OK:
+        raise OracleError(st, f"oracle multi-match hash join status {st}")
+    k = int(n.value)
+    return op[:k], ob[:k]
+
+
 def join_groupby(build_key: HostCol, build_payload: np.ndarray, probe_key: HostCol, value: HostCol | None,
                  max_groups: int = 1 << 16):
     g = np.zeros(max_groups, np.int32)

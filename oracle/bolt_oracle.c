@@ -686,6 +686,54 @@ int orc_hash_join(uint64_t n_build, const orc_col* build_key,
     return cnt > cap ? ORC_CAPACITY : ORC_OK;
 }
 
+typedef struct { uint64_t k; uint32_t row; } krow_t;
+static int cmp_krow(const void* x, const void* y) {
+    const krow_t* a = (const krow_t*)x;
+    const krow_t* b = (const krow_t*)y;
+    if (a->k != b->k) return a->k < b->k ? -1 : 1;
+    return (a->row > b->row) - (a->row < b->row);
+}
+
+/* The map from a key to its build rows in ascending row order is kept as the
+ * valid (key, row) pairs sorted by key then row; a probe key's rows are the
+ * run that a binary search finds. */
+int orc_hash_join_multi(uint64_t n_build, const orc_col* build_key,
+                        uint64_t n_probe, const orc_col* probe_key,
+                        uint32_t* out_probe, uint32_t* out_build, uint64_t cap, uint64_t* n_out) {
+    krow_t* kr = (krow_t*)malloc(sizeof(krow_t) * (n_build ? n_build : 1));
+    if (!kr) return ORC_CAPACITY;
+    uint64_t m = 0;
+    for (uint64_t i = 0; i < n_build; ++i) {
+        uint64_t k;
+        if (!join_key(build_key, i, &k)) continue;  /* NULL keys never match */
+        kr[m].k = k;
+        kr[m].row = (uint32_t)i;
+        ++m;
+    }
+    qsort(kr, m, sizeof(krow_t), cmp_krow);
+    uint64_t cnt = 0;
+    for (uint64_t p = 0; p < n_probe; ++p) {
+        uint64_t k;
+        if (!join_key(probe_key, p, &k)) continue;
+        uint64_t lo = 0, hi = m;  /* first entry with key >= k */
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (kr[mid].k < k) lo = mid + 1;
+            else hi = mid;
+        }
+        for (uint64_t j = lo; j < m && kr[j].k == k; ++j) {
+            if (cnt < cap) {
+                out_probe[cnt] = (uint32_t)p;
+                out_build[cnt] = kr[j].row;
+            }
+            cnt++;
+        }
+    }
+    free(kr);
+    *n_out = cnt;
+    return cnt > cap ? ORC_CAPACITY : ORC_OK;
+}
+
 typedef struct { int32_t g; uint32_t slot; } gslot_t;
 static int cmp_gslot(const void* x, const void* y) {
     int32_t a = ((const gslot_t*)x)->g, b = ((const gslot_t*)y)->g;

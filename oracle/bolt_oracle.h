@@ -76,6 +76,14 @@ int orc_hash_join(uint64_t n_build, const orc_col* build_key,
                   uint64_t n_probe, const orc_col* probe_key,
                   uint32_t* out_probe, uint32_t* out_build, uint64_t cap, uint64_t* n_out);
 
+/* INNER hash join with any build keys, duplicates included: the reference's
+ * host join (join.rs:843-855 build_hash_map keeps each key's build rows in
+ * ascending order; join.rs:407-425 probes in row order and emits one pair per
+ * matching build row). Pairs ordered by probe row, then build row. */
+int orc_hash_join_multi(uint64_t n_build, const orc_col* build_key,
+                        uint64_t n_probe, const orc_col* probe_key,
+                        uint32_t* out_probe, uint32_t* out_build, uint64_t cap, uint64_t* n_out);
+
 /* Join then GROUP BY build payload: SUM(value) (i128, checked add in probe
  * order, aggregate.rs:1220 message) and COUNT(*), sorted by group. */
 int orc_join_groupby(uint64_t n_build, const orc_col* build_key, const int32_t* build_payload,

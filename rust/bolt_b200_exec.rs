@@ -19,8 +19,9 @@
 //     ahead of it, so WHERE + two-key GROUP BY runs here instead of erroring.
 //   * src/exec/join.rs:1336 — `try_gpu_inner_join` calls
 //       try_join_indices_bolt_b200(build_key, probe_key)
-//     for single Int32/Int64 keys before its Stage-1 kernels; `None` keeps
-//     the existing path (duplicate build keys, multi-key, NULLs).
+//     for single Int32/Int64 keys before its Stage-1 and Stage-2 kernels
+//     (duplicate build keys included: every matching build row, ascending);
+//     `None` keeps the existing path (multi-column keys, other dtypes).
 //   * src/exec/sort.rs:191-196 — the `BOLT_GPU_SORT` gate routes through
 //       try_sort_perm_bolt_b200(&batch, sort_exprs)
 //     instead of `try_gpu_sort_radix`; the permutation feeds the same `take`.
@@ -440,8 +441,8 @@ pub fn try_execute_bolt_b200(plan: &PhysicalPlan, batch: &RecordBatch) -> Option
 // ---------------------------------------------------------------------------
 // Hash join indices (replaces Stage 1 of try_gpu_inner_join, join.rs:1336,
 // and gpu_join::hash_join_indices_on_gpu, gpu_join.rs:1403). Pairs come back
-// in probe order. Duplicate build keys decline (None) to the reference's
-// collision-list path.
+// in probe order; a duplicated build key pairs with each of its build rows in
+// ascending order.
 // ---------------------------------------------------------------------------
 pub fn try_join_indices_bolt_b200(build_key: &ArrayRef, probe_key: &ArrayRef)
     -> Option<BoltResult<(UInt32Array, UInt32Array)>> {

@@ -49,8 +49,10 @@ def test_join_key_minus_one_and_duplicates(bolt, engine, oracle):
     pr, br = (x.cpu().numpy().view(np.uint32) for x in
               engine.hash_join_indices(bolt.col(b, "i64").to("cuda"), bolt.col(p, "i64").to("cuda")))
     assert pr.tolist() == [0, 1, 3, 4] and br.tolist() == [2, 0, 0, 1]
-    dup = np.array([1, 2, 1], np.int64)
-    assert engine.hash_join_indices(bolt.col(dup, "i64").to("cuda"), bolt.col(p, "i64").to("cuda")) is None
+    dup = np.array([1, 2, 1, 4, -1, 4], np.int64)
+    pr, br = (x.cpu().numpy().view(np.uint32) for x in
+              engine.hash_join_indices(bolt.col(dup, "i64").to("cuda"), bolt.col(p, "i64").to("cuda")))
+    assert pr.tolist() == [1, 3, 4, 4] and br.tolist() == [4, 4, 3, 5]
 
 
 def test_join_capacity_error(bolt, engine, oracle):
@@ -175,3 +177,34 @@ def test_join_groupby_table_larger_than_l2(bolt, engine, oracle, kdt):
     amt[:, 1] = amt[:, 0] >> 63
     assert -2 not in set(special.tolist())
     _join_groupby_vs_oracle(bolt, engine, oracle, bk, bg, pk, amt, kdt)
+
+
+@pytest.mark.parametrize("dt", ["i32", "i64"])
+@pytest.mark.parametrize("shape", ["few_repeats", "heavy_key", "with_nulls"])
+def test_join_duplicate_build_keys(bolt, engine, oracle, dt, shape):
+    """Build keys that repeat (the reference's collision-list path): every
+    matching build row pairs with the probe row, in probe order and then
+    ascending build row, exactly as the reference's host join map; the
+    output grows past the probe length (the wrapper re-sizes it once)."""
+    rng = np.random.default_rng({"few_repeats": 51, "heavy_key": 52, "with_nulls": 53}[shape])
+    nb, npr = 400_000, 300_000
+    bk = rng.integers(0, 150_000, nb).astype(np.int32 if dt == "i32" else np.int64)
+    bk[::1000] = -1
+    if shape == "heavy_key":
+        bk[rng.random(nb) < 0.05] = 7  # one key with ~20,000 build rows
+    pk = rng.integers(-1000, 160_000, npr).astype(bk.dtype)
+    pk[::997] = -1
+    if shape == "heavy_key":
+        pk[::5000] = 7
+    bvalid = rng.random(nb) > 0.05 if shape == "with_nulls" else None
+    pvalid = rng.random(npr) > 0.05 if shape == "with_nulls" else None
+    b = bolt.col(bk, dt, bitmap(bvalid) if bvalid is not None else None).to("cuda")
+    p = bolt.col(pk, dt, bitmap(pvalid) if pvalid is not None else None).to("cuda")
+    pr, br = (x.cpu().numpy().view(np.uint32) for x in engine.hash_join_indices(b, p))
+    wp, wb = oracle.hash_join_multi(oracle.HostCol(bk, dt, bitmap(bvalid) if bvalid is not None else None),
+                                    oracle.HostCol(pk, dt, bitmap(pvalid) if pvalid is not None else None))
+    assert len(wp) > npr
+    assert np.array_equal(pr, wp) and np.array_equal(br, wb)
+    # The fused join -> GROUP BY needs one build row per key: it declines.
+    assert engine.join_groupby(b, bolt.col(np.zeros(nb, np.int32), "i32").to("cuda"), p,
+                               bolt.col(np.zeros((npr, 2), np.int64), "dec128").to("cuda")) is None

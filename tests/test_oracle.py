@@ -296,3 +296,38 @@ def test_oracle_groupby_par_overflow(oracle):
             oracle.groupby(t, ["k"], [("sum", "v")], threads=threads)
         assert ei.value.status == oracle.OVERFLOW
         assert "SUM(integer) overflow" in str(ei.value)
+
+
+@pytest.mark.parametrize("dt", ["i32", "i64"])
+def test_hash_join_multi_matches_python_dict_join(oracle, dt):
+    """The multi-match join against the reference's host join restated in
+    Python (a dict from key to its build rows in ascending order, probed in
+    row order), with duplicate keys, NULL keys on both sides and key -1; on
+    unique keys it equals the unique-key oracle join."""
+    rng = np.random.default_rng(31)
+    nb, npr = 3000, 5000
+    bk = rng.integers(-40, 400, nb).astype(np.int32 if dt == "i32" else np.int64)
+    bk[::50] = -1
+    pk = rng.integers(-60, 420, npr).astype(bk.dtype)
+    bvalid = rng.random(nb) > 0.05
+    pvalid = rng.random(npr) > 0.05
+    table: dict[int, list[int]] = {}
+    for i in range(nb):
+        if bvalid[i]:
+            table.setdefault(int(bk[i]), []).append(i)
+    want_p, want_b = [], []
+    for p in range(npr):
+        if pvalid[p]:
+            for b in table.get(int(pk[p]), []):
+                want_p.append(p)
+                want_b.append(b)
+
+    def packbits(v):
+        return np.packbits(v.astype(np.uint8), bitorder="little")
+
+    op, ob = oracle.hash_join_multi(oracle.HostCol(bk, dt, packbits(bvalid)), oracle.HostCol(pk, dt, packbits(pvalid)))
+    assert op.tolist() == want_p and ob.tolist() == want_b
+    ub = rng.permutation(np.arange(-500, 500, dtype=bk.dtype))
+    up, ubr = oracle.hash_join_multi(oracle.HostCol(ub, dt), oracle.HostCol(pk, dt))
+    wp, wb = oracle.hash_join(oracle.HostCol(ub, dt), oracle.HostCol(pk, dt))
+    assert np.array_equal(up, wp) and np.array_equal(ubr, wb)
