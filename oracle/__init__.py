@@ -165,6 +165,39 @@ def hash_join(build_key: HostCol, probe_key: HostCol):
     return op[:k], ob[:k]
 
 
+def groupby_wide(table: dict, group_by: list, aggs: list) -> dict:
+    """GROUP BY over two integer key columns wider than 64 bits together (the
+    reference's host wide-key reduction): keys sorted by (key0, key1); per
+    aggregate the values (int64 or float64 by the aggregate's result) and a
+    validity flag."""
+    k0, k1 = table[group_by[0]], table[group_by[1]]
+    n = len(k0.data)
+    na = len(aggs)
+    ops = np.array([AGG[op] for op, _ in aggs], np.int32)
+    ins = (OrcCol * max(na, 1))(*[table[c].c() if c is not None else OrcCol(None, None, 0, 0) for _, c in aggs])
+    cap = max(n, 1)
+    ok0 = np.zeros(cap, np.int64)
+    ok1 = np.zeros(cap, np.int64)
+    oi = np.zeros(na * cap, np.int64)
+    of = np.zeros(na * cap, np.float64)
+    ov = np.zeros(na * cap, np.uint8)
+    ng = C.c_uint64(0)
+    f = lib().orc_groupby_wide
+    f.restype = C.c_int
+    st = f(C.c_uint64(n), C.byref(k0.c()), C.byref(k1.c()), C.c_int32(na), _ptr(ops), ins, _ptr(ok0), _ptr(ok1),
+           _ptr(oi), _ptr(of), _ptr(ov), C.c_uint64(cap), C.byref(ng))
+    if st != OK:
+        raise OracleError(st, f"oracle wide GROUP BY status {st}")
+    g = int(ng.value)
+    vals, valid = [], []
+    for a, (op, c) in enumerate(aggs):
+        in_dt = table[c].dtype if c is not None else None
+        is_f = op == "avg" or (op in ("sum", "min", "max") and in_dt in ("f32", "f64"))
+        vals.append((of if is_f else oi)[a * cap: a * cap + g].copy())
+        valid.append(ov[a * cap: a * cap + g].astype(bool))
+    return {"n_groups": g, "k0": ok0[:g].copy(), "k1": ok1[:g].copy(), "vals": vals, "valid": valid}
+
+
 def hash_join_multi(build_key: HostCol, probe_key: HostCol, cap: int | None = None):
     """INNER join with any build keys (duplicates included): (probe_row,
     build_row) pairs in probe order, then build-row order."""

@@ -686,6 +686,98 @@ int orc_hash_join(uint64_t n_build, const orc_col* build_key,
     return cnt > cap ? ORC_CAPACITY : ORC_OK;
 }
 
+typedef struct { int64_t k0, k1; uint64_t row; } wrow_t;
+static int cmp_wrow(const void* x, const void* y) {
+    const wrow_t* a = (const wrow_t*)x;
+    const wrow_t* b = (const wrow_t*)y;
+    if (a->k0 != b->k0) return a->k0 < b->k0 ? -1 : 1;
+    if (a->k1 != b->k1) return a->k1 < b->k1 ? -1 : 1;
+    return (a->row > b->row) - (a->row < b->row);
+}
+
+static inline int64_t wide_key(const orc_col* c, uint64_t i) {
+    return c->dtype == ORC_I32 ? (int64_t)((const int32_t*)c->data)[i] : ((const int64_t*)c->data)[i];
+}
+
+static inline double num_f64(const orc_col* c, uint64_t i) {
+    switch (c->dtype) {
+    case ORC_I32: return (double)((const int32_t*)c->data)[i];
+    case ORC_I64: return (double)((const int64_t*)c->data)[i];
+    case ORC_F32: return (double)((const float*)c->data)[i];
+    default: return ((const double*)c->data)[i];
+    }
+}
+
+/* The groups are the runs of the rows sorted by (key0, key1, row): equal to
+ * the reference's hash map of tuples sorted by tuple afterwards, and each
+ * run is folded in row order as the reference's row loop folds it. */
+int orc_groupby_wide(uint64_t n, const orc_col* key0, const orc_col* key1, int32_t n_aggs, const int32_t* ops,
+                     const orc_col* inputs, int64_t* out_k0, int64_t* out_k1, int64_t* out_i, double* out_f,
+                     uint8_t* out_valid, uint64_t cap, uint64_t* n_groups) {
+    wrow_t* w = (wrow_t*)malloc(sizeof(wrow_t) * (n ? n : 1));
+    if (!w) return ORC_CAPACITY;
+    uint64_t m = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!is_valid(key0->validity, i) || !is_valid(key1->validity, i)) continue;
+        w[m].k0 = wide_key(key0, i);
+        w[m].k1 = wide_key(key1, i);
+        w[m].row = i;
+        ++m;
+    }
+    qsort(w, m, sizeof(wrow_t), cmp_wrow);
+    uint64_t g = 0;
+    for (uint64_t s = 0; s < m;) {
+        uint64_t e = s + 1;
+        while (e < m && w[e].k0 == w[s].k0 && w[e].k1 == w[s].k1) ++e;
+        if (g < cap) {
+            out_k0[g] = w[s].k0;
+            out_k1[g] = w[s].k1;
+            for (int a = 0; a < n_aggs; ++a) {
+                const orc_col* in = &inputs[a];
+                int64_t ti = 0;
+                double tf = 0.0;
+                uint64_t cnt = 0;
+                int seen = 0;
+                const int is_f = in->data && (in->dtype == ORC_F32 || in->dtype == ORC_F64);
+                for (uint64_t j = s; j < e; ++j) {
+                    const uint64_t r = w[j].row;
+                    if (ops[a] == ORC_COUNT_STAR) { ++cnt; continue; }
+                    if (!is_valid(in->validity, r)) continue;
+                    ++cnt;
+                    if (ops[a] == ORC_SUM) {
+                        if (is_f) tf += num_f64(in, r);
+                        else ti = (int64_t)((uint64_t)ti + (uint64_t)wide_key(in, r));
+                    } else if (ops[a] == ORC_AVG) {
+                        tf += num_f64(in, r);
+                    } else if (ops[a] == ORC_MIN || ops[a] == ORC_MAX) {
+                        if (is_f) {
+                            const double x = num_f64(in, r);
+                            if (!seen || (ops[a] == ORC_MIN ? x < tf : x > tf)) tf = x;
+                        } else {
+                            const int64_t x = wide_key(in, r);
+                            if (!seen || (ops[a] == ORC_MIN ? x < ti : x > ti)) ti = x;
+                        }
+                    }
+                    seen = 1;
+                }
+                uint8_t valid = 1;
+                if (ops[a] == ORC_COUNT_STAR || ops[a] == ORC_COUNT) ti = (int64_t)cnt;
+                else if (ops[a] == ORC_AVG) { valid = cnt > 0; tf = cnt ? tf / (double)cnt : 0.0; }
+                else valid = (uint8_t)seen;
+                if (!valid) { ti = 0; tf = 0.0; }
+                out_i[(uint64_t)a * cap + g] = ti;
+                out_f[(uint64_t)a * cap + g] = tf;
+                out_valid[(uint64_t)a * cap + g] = valid;
+            }
+        }
+        ++g;
+        s = e;
+    }
+    free(w);
+    *n_groups = g;
+    return g > cap ? ORC_CAPACITY : ORC_OK;
+}
+
 typedef struct { uint64_t k; uint32_t row; } krow_t;
 static int cmp_krow(const void* x, const void* y) {
     const krow_t* a = (const krow_t*)x;

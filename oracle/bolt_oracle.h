@@ -76,6 +76,20 @@ int orc_hash_join(uint64_t n_build, const orc_col* build_key,
                   uint64_t n_probe, const orc_col* probe_key,
                   uint32_t* out_probe, uint32_t* out_build, uint64_t cap, uint64_t* n_out);
 
+/* GROUP BY over two integer key columns that do not pack into 64 bits: the
+ * reference's host wide-key reduction (src/exec/groupby_wide.rs:85-262): a
+ * row with a NULL key is dropped; per group and aggregate, in row order,
+ * SUM over integers wraps in i64 (groupby_wide.rs:695-705), SUM / AVG over
+ * floats add in f64, MIN / MAX keep the first valid value and replace it
+ * only when `x < v` / `x > v` (a NaN never replaces a value), COUNT(col)
+ * counts valid inputs; groups ordered by (key0, key1) as signed integers
+ * (cmp_tuple, groupby_wide.rs:410). An aggregate with no valid input in its
+ * group is reported NULL (valid = 0). Per aggregate a: integer results in
+ * out_i[a * cap + g], float results in out_f[a * cap + g]. */
+int orc_groupby_wide(uint64_t n, const orc_col* key0, const orc_col* key1, int32_t n_aggs, const int32_t* ops,
+                     const orc_col* inputs, int64_t* out_k0, int64_t* out_k1, int64_t* out_i, double* out_f,
+                     uint8_t* out_valid, uint64_t cap, uint64_t* n_groups);
+
 /* INNER hash join with any build keys, duplicates included: the reference's
  * host join (join.rs:843-855 build_hash_map keeps each key's build rows in
  * ascending order; join.rs:407-425 probes in row order and emits one pair per

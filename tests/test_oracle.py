@@ -331,3 +331,56 @@ def test_hash_join_multi_matches_python_dict_join(oracle, dt):
     up, ubr = oracle.hash_join_multi(oracle.HostCol(ub, dt), oracle.HostCol(pk, dt))
     wp, wb = oracle.hash_join(oracle.HostCol(ub, dt), oracle.HostCol(pk, dt))
     assert np.array_equal(up, wp) and np.array_equal(ubr, wb)
+
+
+def test_groupby_wide_matches_python_reduction(oracle):
+    """The wide-key oracle against the reference's host wide reduction
+    restated in Python: NULL-key rows dropped, wrapping int64 SUM, f64 SUM and
+    AVG in row order, first-seen MIN / MAX, COUNT of valid inputs, groups in
+    (key0, key1) order."""
+    rng = np.random.default_rng(61)
+    n = 20_000
+    k0 = rng.integers(-5, 6, n).astype(np.int64) * (2 ** 40)
+    k1 = rng.integers(-300, 300, n).astype(np.int32)
+    vi = rng.integers(-2 ** 62, 2 ** 62, n)
+    vd = rng.normal(0, 1e3, n)
+    v32 = rng.integers(-1000, 1000, n).astype(np.int32)
+    kv = rng.random(n) > 0.03
+    vv = rng.random(n) > 0.2
+
+    def bm(v):
+        return np.packbits(v.astype(np.uint8), bitorder="little")
+
+    table = {"k0": oracle.HostCol(k0, "i64", bm(kv)), "k1": oracle.HostCol(k1, "i32"),
+             "vi": oracle.HostCol(vi, "i64", bm(vv)), "vd": oracle.HostCol(vd, "f64", bm(vv)),
+             "v32": oracle.HostCol(v32, "i32")}
+    aggs = [("sum", "vi"), ("sum", "vd"), ("avg", "v32"), ("count_star", None), ("count", "vi"),
+            ("min", "vd"), ("max", "vi"), ("min", "v32")]
+    r = oracle.groupby_wide(table, ["k0", "k1"], aggs)
+    groups: dict = {}
+    for i in range(n):
+        if kv[i]:
+            groups.setdefault((int(k0[i]), int(k1[i])), []).append(i)
+    keys = sorted(groups)
+    assert r["n_groups"] == len(keys)
+    assert r["k0"].tolist() == [k[0] for k in keys] and r["k1"].tolist() == [k[1] for k in keys]
+    for g, key in enumerate(keys):
+        rows = groups[key]
+        vrows = [i for i in rows if vv[i]]
+        s = 0
+        for i in vrows:
+            s = (s + int(vi[i]) + 2 ** 63) % 2 ** 64 - 2 ** 63
+        assert r["vals"][0][g] == s and r["valid"][0][g] == bool(vrows)
+        fs = 0.0
+        for i in vrows:
+            fs += float(vd[i])
+        assert (r["vals"][1][g] == fs) if vrows else not r["valid"][1][g]
+        a = 0.0
+        for i in rows:
+            a += float(v32[i])
+        assert r["vals"][2][g] == a / len(rows)
+        assert r["vals"][3][g] == len(rows) and r["vals"][4][g] == len(vrows)
+        if vrows:
+            assert r["vals"][5][g] == min(float(vd[i]) for i in vrows)
+            assert r["vals"][6][g] == max(int(vi[i]) for i in vrows)
+        assert r["vals"][7][g] == min(int(v32[i]) for i in rows)
