@@ -230,7 +230,7 @@ class Engine:
     @property
     def last_groupby_tier(self) -> int:
         """Tier of the last GROUP BY: 1 shared-memory + global hash table,
-        2 hash-partitioned."""
+        2 hash-partitioned, 3 the sort-based path for keys wider than 64 bits."""
         return int(self._lib.bolt_ctx_last_groupby_tier(self._ctx))
 
     @property

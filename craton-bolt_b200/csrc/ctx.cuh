@@ -32,7 +32,7 @@ struct bolt_ctx {
     uint32_t kcount = 0;
     double last_ms = 0.0;
     uint32_t last_launches = 0;
-    int32_t last_tier = 0;       // GROUP BY tier of the last bolt_groupby (1 global table, 2 partitioned)
+    int32_t last_tier = 0;       // GROUP BY tier of the last bolt_groupby (1 global table, 2 partitioned, 3 wide keys)
     uint32_t async_pending = 0;
     std::string last_error;
     // Pinned staging ring for descriptor uploads: each upload copies into the

@@ -2052,6 +2052,7 @@ extern "C" bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc
     uint64_t nrows = 0;
     if (desc->n_keys >= 1 && desc->key_cols && desc->cols && desc->key_cols[0] >= 0 && desc->key_cols[0] < desc->n_cols)
         nrows = desc->cols[desc->key_cols[0]].len;
+    if (gb_wide_applies(desc)) return gb_wide(ctx, desc, out, flags, (cudaStream_t)stream);
     return gb_single(ctx, desc, out, 0, nrows, flags, (cudaStream_t)stream, nullptr, nullptr, "GROUP BY");
 }
 

@@ -200,6 +200,12 @@ struct GbStagedLaunch {
     int smem_log2;
     size_t smem;
 };
+// GROUP BY over two integer key columns at least one of which is Int64 (keys
+// that do not pack into 64 bits), without WHERE: sort-based, synchronous.
+bool gb_wide_applies(const bolt_groupby_desc* d);
+bolt_status gb_wide(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_groupby_out* out, uint32_t flags,
+                    cudaStream_t s);
+
 bool gb_staged_layout(const bolt_ctx* ctx, const GbPlan& plan, GbStagedLaunch* out);
 
 // Allocates scratch and enqueues table init, aggregation and finalize of

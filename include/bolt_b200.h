@@ -118,7 +118,8 @@ double      bolt_ctx_last_device_ms(const bolt_ctx* ctx);
 uint32_t    bolt_ctx_last_launches(const bolt_ctx* ctx);
 /* Which GROUP BY tier served the last bolt_groupby on this context: 1 = the
  * shared-memory tier over a global hash table, 2 = the hash-partitioned tier
- * (the reference's Tier-1 / Tier-2 executors); 0 before any GROUP BY. */
+ * (the reference's Tier-1 / Tier-2 executors), 3 = the sort-based wide-key
+ * path (groupby_wide.rs); 0 before any GROUP BY. */
 int32_t     bolt_ctx_last_groupby_tier(const bolt_ctx* ctx);
 /* Device milliseconds of the dominant kernel of every call made with
  * BOLT_FLAG_PROFILE or BOLT_FLAG_KERNEL_TIMES since the previous read (up to 256 calls, oldest first).
@@ -145,6 +146,14 @@ const char* bolt_version(void);
 /*         exactly as pack_keys (groupby_common.rs:352): I32 sign-extended,  */
 /*         (I32,I32) -> (a << 32) | (u32)b, floats by bit pattern after      */
 /*         -0.0 -> +0.0 and NaN -> one canonical NaN;                         */
+/*   wide keys: 2 integer columns with at least one I64 (no 64-bit packing)  */
+/*         follow the reference's host wide reduction (groupby_wide.rs:85):  */
+/*         synchronous calls without WHERE only; rows with a NULL in either  */
+/*         key are dropped; groups sorted by (key0, key1) as signed integers; */
+/*         each aggregate is a row-order fold (integer SUM wraps in i64, SUM/ */
+/*         AVG over F64 add in order, MIN/MAX keep the first valid value and */
+/*         replace it on < / >, so a NaN replaces nothing); SUM/AVG over     */
+/*         I32/I64/F64 and MIN/MAX over I32/I64/F32/F64, else BOLT_DECLINE;  */
 /*   output rows sorted by the packed key as a signed 64-bit integer,        */
 /*         ascending (groupby.rs:789-800); rows with a NULL key (single-key   */
 /*         only) form one group emitted last with a NULL key;                 */

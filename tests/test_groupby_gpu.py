@@ -323,9 +323,9 @@ def test_groupby_where_float_and_multiple_conjuncts(bolt, engine, oracle):
 
 
 def test_groupby_decline_unsupported(bolt, engine, oracle):
-    k = np.zeros(4, np.int64)
+    k = np.zeros(4, np.float64)
     v = np.zeros(4, np.int64)
-    dev, _ = tables(bolt, oracle, {"a": (k, None, "i64", 0), "b": (v, None, "i64", 0)})
+    dev, _ = tables(bolt, oracle, {"a": (k, None, "f64", 0), "b": (v, None, "i64", 0)})
     assert engine.try_execute_groupby(dev, ["a", "b"], [("count_star", None)]) is None
 
 
