@@ -1916,6 +1916,38 @@ static bolt_status gb_host(bolt_ctx* ctx, const bolt_groupby_desc* d, bolt_group
         if (d->cols[i].len < n) return fail(ctx, BOLT_ERR_INVALID, "%s: column %d shorter than the key", op, i);
         row_bytes += (uint64_t)w + (d->cols[i].validity ? 1 : 0);
     }
+    if (gb_wide_applies(d)) {
+        // Keys wider than 64 bits: the sort-based path needs every row at
+        // once, so the used columns are uploaded whole into the arena, held
+        // there (pinned) while the wide path runs on the device copies.
+        const uint64_t pinned0 = ctx->arena_pinned;
+        ctx->arena_used = pinned0;
+        std::vector<bolt_col_view> dev(d->cols, d->cols + d->n_cols);
+        for (int i = 0; i < d->n_cols; ++i) {
+            if (!used[i]) continue;
+            const uint64_t db = n * (uint64_t)dtype_width(d->cols[i].dtype);
+            const uint64_t vb = (n + 7) / 8;
+            void* dd = arena_alloc(ctx, db ? db : 1);
+            uint8_t* dv = d->cols[i].validity ? (uint8_t*)arena_alloc(ctx, vb ? vb : 1) : nullptr;
+            if (!dd || (d->cols[i].validity && !dv))
+                return fail(ctx, BOLT_ERR_CAPACITY, "%s: scratch arena too small for the wide-key columns", op);
+            if (db) BOLT_CUDA(ctx, cudaMemcpyAsync(dd, d->cols[i].data, db, cudaMemcpyHostToDevice, s));
+            if (dv && vb) BOLT_CUDA(ctx, cudaMemcpyAsync(dv, d->cols[i].validity, vb, cudaMemcpyHostToDevice, s));
+            dev[i].data = dd;
+            dev[i].validity = dv;
+            dev[i].len = n;
+        }
+        bolt_groupby_desc dd = *d;
+        dd.cols = dev.data();
+        ctx->arena_pinned = ctx->arena_used;
+        const bolt_status st = gb_wide(ctx, &dd, out, flags, s);
+        // The copies and kernels are done before the columns are unpinned
+        // and before the caller's host buffers may be reused.
+        const cudaError_t e = cudaStreamSynchronize(s);
+        ctx->arena_pinned = pinned0;
+        if (st == BOLT_OK && e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
+        return st;
+    }
     constexpr int NB = bolt_ctx::HOST_SLOTS;
     if (!ctx->copy_stream) {
         BOLT_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -25,6 +25,7 @@
 // GROUP BY path of this library; the reference emits the accumulator's
 // initial value (0 for SUM and AVG, the type's extreme for MIN / MAX).
 #include <algorithm>
+#include <climits>
 
 #include "compact.cuh"
 #include "groupby.cuh"
@@ -93,10 +94,35 @@ __global__ void __launch_bounds__(256) wide_mark_kernel(const void* k0, int dt0,
     }
 }
 
+constexpr int WIDE_PF = 4;  // 32-row chunks of a fold in flight per warp
+
+// One lane's element of a 32-row chunk of a group: validity and value.
+struct WideElem {
+    bool v;
+    ll xi;
+    double xf;
+};
+
+__device__ __forceinline__ WideElem wide_elem(const WideArgs& a, const WideAgg& w, uint64_t j, uint64_t end) {
+    WideElem e = {false, 0, 0.0};
+    if (j < end) {
+        const uint32_t r = a.perm[j];
+        e.v = bit_valid(w.in_valid, r);
+        if (e.v && w.op != BOLT_AGG_COUNT) {
+            if (w.fold_f) e.xf = wide_load_f(w.in, w.in_dtype, r);
+            else e.xi = wide_load_i(w.in, w.in_dtype, r);
+        }
+    }
+    return e;
+}
+
 // One warp per group: the group's keys from its first row, then every
-// aggregate folded over the group's rows in row order. Each 32-row chunk is
-// loaded by the lanes together; the fold then walks the valid lanes in order
-// through shuffles, every lane keeping the same accumulator.
+// aggregate over the group's rows. Integer aggregates (wrapping SUM, COUNT,
+// MIN / MAX) do not depend on the order: each lane folds its own rows
+// (WIDE_PF chunks loaded at a time) and the warp reduces at the end. Float
+// aggregates fold in row order: each 32-row chunk is loaded by the lanes
+// together (WIDE_PF chunks ahead of the fold), then every lane walks the
+// chunk's 32 values in order through shuffles, keeping the same accumulator.
 __global__ void __launch_bounds__(256) wide_fold_kernel(const __grid_constant__ WideArgs a) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -119,38 +145,66 @@ __global__ void __launch_bounds__(256) wide_fold_kernel(const __grid_constant__ 
             bool seen = false;
             if (w.op == BOLT_AGG_COUNT_STAR) {
                 cnt = end - beg;
-            } else {
-                for (uint64_t c = beg; c < end; c += 32) {
-                    const uint64_t j = c + lane;
-                    bool v = false;
-                    ll xi = 0;
-                    double xf = 0.0;
-                    if (j < end) {
-                        const uint32_t r = a.perm[j];
-                        v = bit_valid(w.in_valid, r);
-                        if (v && w.op != BOLT_AGG_COUNT) {
-                            if (w.fold_f) xf = wide_load_f(w.in, w.in_dtype, r);
-                            else xi = wide_load_i(w.in, w.in_dtype, r);
+            } else if (!w.fold_f) {
+                const bool is_min = w.op == BOLT_AGG_MIN;
+                ll lm = is_min ? LLONG_MAX : LLONG_MIN;
+                bool lseen = false;
+                for (uint64_t c = beg; c < end; c += 32 * WIDE_PF) {
+                    WideElem e[WIDE_PF];  // every load of WIDE_PF chunks issued before any is used
+#pragma unroll
+                    for (int p = 0; p < WIDE_PF; ++p) e[p] = wide_elem(a, w, c + (uint64_t)p * 32 + lane, end);
+#pragma unroll
+                    for (int p = 0; p < WIDE_PF; ++p) {
+                        cnt += (uint64_t)__popc(__ballot_sync(0xffffffffu, e[p].v));
+                        if (e[p].v) {
+                            si += (ull)e[p].xi;
+                            lm = is_min ? (e[p].xi < lm ? e[p].xi : lm) : (e[p].xi > lm ? e[p].xi : lm);
+                            lseen = true;
                         }
-                    }
-                    unsigned m = __ballot_sync(0xffffffffu, v);
-                    cnt += (uint64_t)__popc(m);
-                    if (w.op == BOLT_AGG_COUNT) continue;
-                    while (m) {  // warp-uniform: m is a ballot
-                        const int t = __ffs(m) - 1;
-                        m &= m - 1;
-                        if (w.fold_f) {
-                            const double x = __shfl_sync(0xffffffffu, xf, t);
-                            if (w.op == BOLT_AGG_SUM || w.op == BOLT_AGG_AVG) f += x;
-                            else if (!seen || (w.op == BOLT_AGG_MIN ? x < f : x > f)) f = x;
-                        } else {
-                            const ll x = __shfl_sync(0xffffffffu, xi, t);
-                            if (w.op == BOLT_AGG_SUM) si += (ull)x;
-                            else if (!seen || (w.op == BOLT_AGG_MIN ? x < mi : x > mi)) mi = x;
-                        }
-                        seen = true;
                     }
                 }
+                seen = __any_sync(0xffffffffu, lseen);
+                for (int o = 16; o > 0; o >>= 1) {
+                    si += __shfl_xor_sync(0xffffffffu, si, o);
+                    const ll y = __shfl_xor_sync(0xffffffffu, lm, o);
+                    lm = is_min ? (y < lm ? y : lm) : (y > lm ? y : lm);
+                }
+                mi = lm;
+            } else {
+                const int kind = (w.op == BOLT_AGG_SUM || w.op == BOLT_AGG_AVG) ? 0 : (w.op == BOLT_AGG_MIN ? 1 : 2);
+                // WIDE_PF chunks in flight: chunk i + WIDE_PF is loaded
+                // before chunk i is folded. Lanes past the group's end load
+                // nothing and hold no valid value.
+                WideElem buf[WIDE_PF];
+#pragma unroll
+                for (int p = 0; p < WIDE_PF; ++p) buf[p] = wide_elem(a, w, beg + (uint64_t)p * 32 + lane, end);
+                for (uint64_t c = beg; c < end; c += 32 * WIDE_PF) {
+#pragma unroll
+                    for (int p = 0; p < WIDE_PF; ++p) {
+                        const WideElem e = buf[p];
+                        buf[p] = wide_elem(a, w, c + (uint64_t)(p + WIDE_PF) * 32 + lane, end);
+                        const unsigned m = __ballot_sync(0xffffffffu, e.v);
+                        if (m == 0) continue;  // warp-uniform
+                        cnt += (uint64_t)__popc(m);
+                        if (kind == 0) {
+#pragma unroll
+                            for (int t = 0; t < 32; ++t) {
+                                const double x = __shfl_sync(0xffffffffu, e.xf, t);
+                                f = ((m >> t) & 1) ? f + x : f;
+                            }
+                        } else {
+#pragma unroll
+                            for (int t = 0; t < 32; ++t) {
+                                const double x = __shfl_sync(0xffffffffu, e.xf, t);
+                                const bool on = (m >> t) & 1;
+                                const bool take = on && (!seen || (kind == 1 ? x < f : x > f));
+                                f = take ? x : f;
+                                seen = seen || on;
+                            }
+                        }
+                    }
+                }
+                if (kind == 0) seen = cnt > 0;
             }
             if (lane != 0) continue;
             bool valid = true;

@@ -225,7 +225,9 @@ bolt_status bolt_groupby(bolt_ctx* ctx, const bolt_groupby_desc* desc,
  * transfer and aggregation overlap and no column is resident in full.
  * Always synchronises (BOLT_FLAG_ASYNC -> BOLT_ERR_INVALID). A query whose
  * SUM(Int64) needs the row-order overflow check returns BOLT_DECLINE: run it
- * on device columns through bolt_groupby. */
+ * on device columns through bolt_groupby. Keys wider than 64 bits (the wide
+ * form above) sort every row at once: their columns are uploaded whole, not
+ * streamed. */
 bolt_status bolt_groupby_host(bolt_ctx* ctx, const bolt_groupby_desc* desc,
                               bolt_groupby_out* out, uint32_t flags, bolt_stream stream);
 

@@ -108,3 +108,16 @@ def test_groupby_wide_keys_edge_cases(bolt, engine, oracle):
     assert engine.try_execute_groupby(dev, ["k0", "k1"], AGGS, flags=bolt.FLAG_ASYNC) is None
     # SUM over Float32 has no wide-key form.
     assert engine.try_execute_groupby(dev, ["k0", "k1"], [("sum", "vf")]) is None
+
+
+def test_groupby_wide_keys_host_columns(bolt, engine, oracle):
+    """Host columns through bolt_groupby_host (the reference's RecordBatch
+    entry): uploaded whole, then the same wide path; host results equal to the
+    oracle."""
+    rng = np.random.default_rng(17)
+    cols = _columns(rng, 200_003, ("i32", "i64"), 300, key_nulls=True)
+    host_cols = {name: bolt.col(d, dt, v) for name, (d, v, dt) in cols.items()}
+    res = engine.execute_groupby(host_cols, ["k0", "k1"], AGGS)
+    assert not res.keys[0].is_cuda and engine.last_groupby_tier == 3
+    host = {name: oracle.HostCol(d, dt, v) for name, (d, v, dt) in cols.items()}
+    _check(res, oracle.groupby_wide(host, ["k0", "k1"], AGGS), AGGS)
