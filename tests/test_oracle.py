@@ -384,3 +384,29 @@ def test_groupby_wide_matches_python_reduction(oracle):
             assert r["vals"][5][g] == min(float(vd[i]) for i in vrows)
             assert r["vals"][6][g] == max(int(vi[i]) for i in vrows)
         assert r["vals"][7][g] == min(int(v32[i]) for i in rows)
+
+
+def test_groupby_wide_edge_cases(oracle):
+    """No rows, every key NULL, and a group whose inputs are all NULL (NULL
+    SUM / MIN / AVG, COUNT 0, COUNT(*) the row count)."""
+    e = np.zeros(0, np.int64)
+    r = oracle.groupby_wide({"a": oracle.HostCol(e, "i64"), "b": oracle.HostCol(e, "i64")}, ["a", "b"],
+                            [("count_star", None)])
+    assert r["n_groups"] == 0
+    k = np.arange(8, dtype=np.int64)
+    none = np.packbits(np.zeros(8, np.uint8), bitorder="little")
+    r = oracle.groupby_wide({"a": oracle.HostCol(k, "i64", none), "b": oracle.HostCol(k, "i64")}, ["a", "b"],
+                            [("count_star", None)])
+    assert r["n_groups"] == 0
+    v = np.array([5, 6, 7, 8, 9, 10, 11, 12], np.int64)
+    vv = np.packbits(np.array([0, 0, 0, 0, 1, 1, 1, 1], np.uint8), bitorder="little")
+    keys = np.array([1, 1, 1, 1, 2, 2, 2, 2], np.int64)
+    t = {"a": oracle.HostCol(keys, "i64"), "b": oracle.HostCol(np.zeros(8, np.int32), "i32"),
+         "v": oracle.HostCol(v, "i64", vv)}
+    aggs = [("sum", "v"), ("min", "v"), ("avg", "v"), ("count", "v"), ("count_star", None)]
+    r = oracle.groupby_wide(t, ["a", "b"], aggs)
+    assert r["n_groups"] == 2 and r["k0"].tolist() == [1, 2]
+    assert [x[0] for x in r["valid"]] == [False, False, False, True, True]
+    assert [x[1] for x in r["valid"]] == [True] * 5
+    assert [int(x[1]) if i != 2 else float(x[1]) for i, x in enumerate(r["vals"])] == [42, 9, 10.5, 4, 4]
+    assert r["vals"][3][0] == 0 and r["vals"][4][0] == 4
