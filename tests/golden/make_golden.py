@@ -205,11 +205,33 @@ sort = [
 ]
 
 
+groupby_wide = []
+# groupby_wide.rs:1404-1436 (two_int64_keys_sum_count_avg): three (a, b) tuples, output sorted by (a, b)
+_rows = [(1, 10, 100), (2, 10, 7), (1, 20, 50), (1, 10, 200), (2, 10, 8), (2, 10, 9)]
+groupby_wide.append({
+    "name": "two_int64_keys_sum_count_avg", "source": "src/exec/groupby_wide.rs:1404-1436",
+    "columns": {"a": c("i64", [r[0] for r in _rows]), "b": c("i64", [r[1] for r in _rows]),
+                "v": c("i64", [r[2] for r in _rows])},
+    "group_by": ["a", "b"], "aggs": [["sum", "v"], ["count", "v"], ["avg", "v"]],
+    "expected": {"k0": [1, 1, 2], "k1": [10, 20, 10], "aggs": [[300, 50, 24], [2, 1, 3], [150.0, 50.0, 8.0]]},
+})
+# groupby_wide.rs:1438-1471 (deterministic_ordering): a in 0..20, b in 0..5, v = a * 100 + b, one row
+# per (a, b); the test asserts 100 groups in (a, b) order, so each group's SUM and AVG are its v.
+_rows = [(a, b, a * 100 + b) for a in range(20) for b in range(5)]
+groupby_wide.append({
+    "name": "deterministic_ordering", "source": "src/exec/groupby_wide.rs:1438-1471",
+    "columns": {"a": c("i64", [r[0] for r in _rows]), "b": c("i64", [r[1] for r in _rows]),
+                "v": c("i64", [r[2] for r in _rows])},
+    "group_by": ["a", "b"], "aggs": [["sum", "v"], ["count", "v"], ["avg", "v"]],
+    "expected": {"k0": [r[0] for r in _rows], "k1": [r[1] for r in _rows],
+                 "aggs": [[r[2] for r in _rows], [1] * len(_rows), [float(r[2]) for r in _rows]]},
+})
+
 def main():
     doc = {"about": "known answers transcribed from the reference's tests for this path",
-           "groupby": groupby, "join": join, "sort_keys": sort_keys, "sort": sort}
+           "groupby": groupby, "groupby_wide": groupby_wide, "join": join, "sort_keys": sort_keys, "sort": sort}
     OUT.write_text(json.dumps(doc, indent=1, default=lambda x: None) + "\n")
-    print(f"wrote {OUT} ({len(groupby)} groupby, {len(join)} join, {len(sort_keys)} sort-key, {len(sort)} sort)")
+    print(f"wrote {OUT} ({len(groupby)} groupby, {len(groupby_wide)} wide groupby, {len(join)} join, {len(sort_keys)} sort-key, {len(sort)} sort)")
 
 
 if __name__ == "__main__":

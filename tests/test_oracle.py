@@ -410,3 +410,14 @@ def test_groupby_wide_edge_cases(oracle):
     assert [x[1] for x in r["valid"]] == [True] * 5
     assert [int(x[1]) if i != 2 else float(x[1]) for i, x in enumerate(r["vals"])] == [42, 9, 10.5, 4, 4]
     assert r["vals"][3][0] == 0 and r["vals"][4][0] == 4
+
+
+@pytest.mark.parametrize("case", golden()["groupby_wide"], ids=lambda c: c["name"])
+def test_oracle_groupby_wide_known_answers(oracle, case):
+    """The wide-key oracle against the reference's own wide GROUP BY tests."""
+    t = host_table(oracle, case["columns"])
+    exp = case["expected"]
+    r = oracle.groupby_wide(t, case["group_by"], [tuple(a) for a in case["aggs"]])
+    assert r["k0"].tolist() == exp["k0"] and r["k1"].tolist() == exp["k1"]
+    for a, want in enumerate(exp["aggs"]):
+        assert r["vals"][a].tolist() == want and r["valid"][a].all()
