@@ -13,7 +13,10 @@
 //     spill:` error, which `try_fast_path!` (groupby.rs:329-354) treats as a
 //     soft miss and falls through, exactly like the reference's Tier-2
 //     reduce; BOLT_DECLINE is `None` (next strategy); every other error
-//     propagates.
+//     propagates. Two integer keys wider than 64 bits (an Int64 among them,
+//     no WHERE) take the library's sort-based wide form through the same
+//     call, ahead of the host reducer at groupby.rs:513-522; other wide
+//     shapes decline to it.
 //   * src/exec/groupby_with_pre.rs:248-252 — the multi-column reject becomes
 //       if let Some(r) = crate::exec::bolt_b200_exec::try_execute_bolt_b200(plan, table_batch) { return r; }
 //     ahead of it, so WHERE + two-key GROUP BY runs here instead of erroring.
